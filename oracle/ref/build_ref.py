@@ -1,0 +1,127 @@
+"""Build the reference's own CPU path (cuFE src/*.c, compiled unmodified from where the
+sources lie under /root/reference) into oracle/_ref/<variant>/libref.so.
+
+TEST INFRASTRUCTURE ONLY: the resulting libraries are the pinned oracle that the C
+restatement (oracle/cufe_oracle.c) and the golden fixtures are checked against, and the
+CPU baseline timed by bench.py --impl reference.
+
+Recipe (no copying of reference sources; outputs only under oracle/_ref/):
+  * the reference headers are used as shipped for the `default` variant (n=4096, l=785);
+    other (n, l) variants pre-include a generated params/consts header (-include) whose
+    include guards (PARAMS_H, CONSTS_H) turn the shipped params.h/consts.h into no-ops;
+  * <gmp.h> is the declaration shim in oracle/ref/shim, linked to the system libgmp.so.10;
+  * src/randombytes.c is replaced by oracle/ref/ref_glue.c (queued seeds) at link time;
+  * -ftrivial-auto-var-init=zero makes the never-initialised AES contexts of
+    rlwe_sife_setup/encrypt deterministic (all-zero round keys, counter 0);
+  * -O3 with AVX2/FMA/AES-NI (the reference Makefile uses -march=native -mavx2; the
+    explicit x86-64-v3 target keeps the library runnable on any AVX2 host and keeps
+    the FMA contraction of the Bernoulli polynomial that -march=native gives).
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE = os.path.dirname(HERE)
+OUT = os.path.join(ORACLE, "_ref")
+REF = os.environ.get("CUFE_REFERENCE_ROOT", "/root/reference")
+SRC = os.path.join(REF, "src")
+UNITS = ["aes256ctr.c", "arith_rns.c", "crt.c", "gauss.c", "ntt.c", "rlwe_sife.c", "sample.c"]
+CFLAGS = ["-O3", "-fomit-frame-pointer", "-march=x86-64-v3", "-maes", "-fPIC", "-w",
+          "-ftrivial-auto-var-init=zero"]
+
+Q = [16760833, 2147352577, 2130706433]
+PSI8192 = [3689, 1689795, 456478]
+VARIANTS = {  # name -> (n, l); None = shipped headers
+    "default": None,
+    "n4096_l784": (4096, 784),
+    "n2048_l124": (2048, 124),
+    "n1024_l16": (1024, 16),
+    "n256_l8": (256, 8),
+}
+
+
+def _bitrev(x, bits):
+    return int(format(x, "0%db" % bits)[::-1], 2) if bits else 0
+
+
+def _root(j, n):
+    q = Q[j]
+    if 2 * n <= 8192:
+        return pow(PSI8192[j], 8192 // (2 * n), q)
+    raise ValueError("variants above n=4096 are not built")
+
+
+def gen_headers(n, l, d):
+    qfull = Q[0] * Q[1] * Q[2]
+    p = 64 * l + 1
+    delta = qfull // p
+    c1 = pow(Q[0], -1, Q[1])
+    c2 = pow(Q[0] * Q[1], -1, Q[2])
+    with open(os.path.join(d, "gen_params.h"), "w") as f:
+        f.write("/* generated by oracle/ref/build_ref.py: n=%d l=%d */\n" % (n, l))
+        f.write("#ifndef PARAMS_H\n#define PARAMS_H\n#include <stdint.h>\n#include <stdlib.h>\n")
+        f.write("#define Malloc(type,n) (type *)malloc((n)*sizeof(type))\n")
+        f.write("#define max_data 1\n#define CLOCKS_PER_MS 2700000\n#define PERF\n#define CPU\n#define GPU\n")
+        f.write('static const char SIFE_Q_str[] = "%d";\n' % qfull)
+        f.write("#define SIFE_LOGQ_BYTE 88\n#define SIFE_NMODULI 3\n")
+        f.write("static const uint64_t SIFE_CRT_CONSTS[SIFE_NMODULI]={0, %d, %d};\n" % (c1, c2))
+        f.write("static const uint32_t SIFE_MOD_Q_I[SIFE_NMODULI] = {%d, %d, %d};\n" % tuple(Q))
+        f.write("#define SIFE_B_x 4\n#define SIFE_B_y 16\n#define SIFE_L %d\n#define SIFE_N %d\n" % (l, n))
+        f.write("#define SIFE_SIGMA 1\n")
+        f.write('static const char SIFE_P_str[] = "%d";\n' % p)
+        f.write('static const char SIFE_SCALE_M_str[]="%d";\n' % delta)
+        f.write("static const uint64_t SIFE_SCALE_M_MOD_Q_I[SIFE_NMODULI]={%d, %d, %d};\n"
+                % tuple(delta % q for q in Q))
+        f.write("#endif\n")
+    logn = n.bit_length() - 1
+    with open(os.path.join(d, "gen_consts.h"), "w") as f:
+        f.write("/* generated by oracle/ref/build_ref.py: n=%d */\n" % n)
+        f.write("#ifndef CONSTS_H\n#define CONSTS_H\n#include <stdint.h>\n")
+        f.write("static const uint32_t SIFE_NTT_NINV[SIFE_NMODULI]={%s};\n"
+                % ", ".join(str(pow(n, -1, q)) for q in Q))
+        for name, sign in (("psi", 1), ("psi_inv", -1)):
+            rows = []
+            for j, q in enumerate(Q):
+                w = pow(_root(j, n), sign, q)
+                rows.append("{" + ", ".join(str(pow(w, _bitrev(k, logn), q)) for k in range(n)) + "}")
+            f.write("uint32_t %s[SIFE_NMODULI][SIFE_N] = {%s};\n" % (name, ",\n".join(rows)))
+        f.write("#endif\n")
+
+
+def build_variant(name, dims, force=False):
+    d = os.path.join(OUT, name)
+    lib = os.path.join(d, "libref.so")
+    if os.path.exists(lib) and not force:
+        return lib
+    os.makedirs(d, exist_ok=True)
+    pre = []
+    if dims is not None:
+        gen_headers(dims[0], dims[1], d)
+        pre = ["-include", os.path.join(d, "gen_params.h")]
+    inc = ["-I", SRC, "-I", os.path.join(HERE, "shim")]
+    objs = []
+    for unit in UNITS + ["GLUE"]:
+        src = os.path.join(HERE, "ref_glue.c") if unit == "GLUE" else os.path.join(SRC, unit)
+        obj = os.path.join(d, os.path.basename(src) + ".o")
+        extra = list(pre)
+        if dims is not None and unit == "ntt.c":
+            extra += ["-include", os.path.join(d, "gen_consts.h")]
+        cmd = ["gcc", "-c", src, "-o", obj] + CFLAGS + extra + inc
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    subprocess.run(["gcc", "-shared", "-o", lib] + objs + ["-l:libgmp.so.10", "-lm"], check=True)
+    return lib
+
+
+def build_all(force=False):
+    if not os.path.isdir(SRC):
+        return False
+    for name, dims in VARIANTS.items():
+        build_variant(name, dims, force)
+    return True
+
+
+if __name__ == "__main__":
+    ok = build_all(force="--force" in sys.argv)
+    print("built" if ok else "reference sources absent; nothing built")
