@@ -1,0 +1,290 @@
+"""cufe_b200: B200-native (sm_100a) RLWE inner-product functional encryption.
+
+Python binding over the C ABI of libcufe_b200.so (include/cufe_b200.h).  Device buffers are
+torch CUDA tensors (plumbing only); every computation runs in the library's own kernels.
+There is no CPU fallback: importing works without a GPU, but every compute call needs the
+shared library and a CUDA device and raises otherwise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcufe_b200.so")
+
+OK = 0
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
+          -4: "sampler status set", -5: "no CUDA device"}
+SIGMA1, SIGMA2, SIGMA3 = 0, 1, 2
+Q = (16760833, 2147352577, 2130706433)
+
+_lib = None
+
+
+class CufeError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        msg = _lib.cufe_last_error().decode() if _lib is not None else ""
+        super().__init__("%s: %s (%d) %s" % (what, ERRORS.get(code, "error"), code, msg))
+
+
+def build(force=False):
+    """Compile the CUDA sources into the in-tree shared library."""
+    from . import build as _b
+    return _b.build(force=force)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libcufe_b200.so is not built (python -m cufe_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        vp, i, ll = C.c_void_p, C.c_int, C.c_longlong
+        L.cufe_last_error.restype = C.c_char_p
+        L.cufe_version.restype = C.c_char_p
+        sig = {
+            "cufe_create": [C.POINTER(vp), i, i, i],
+            "cufe_destroy": [vp],
+            "cufe_sync": [vp, vp],
+            "cufe_ctx_stream": [vp],
+            "cufe_params": [vp, vp, vp],
+            "cufe_tables": [vp, vp, vp],
+            "cufe_setup": [vp, vp, vp, vp, vp, vp, vp],
+            "cufe_setup_gpu_map": [vp, vp, vp, vp, vp, vp],
+            "cufe_encrypt": [vp, i, vp, vp, vp, vp, vp, vp],
+            "cufe_encrypt_gpu_map": [vp, i, vp, vp, vp, vp, vp],
+            "cufe_keygen": [vp, i, vp, i, vp, vp, vp],
+            "cufe_decrypt": [vp, i, vp, i, vp, i, vp, vp, vp],
+            "cufe_decode": [vp, i, vp, i, vp, vp],
+            "cufe_sample_cpu_map": [vp, i, i, vp, i, vp, vp],
+            "cufe_sample_gpu_map": [vp, i, vp, i, i, vp, vp],
+            "cufe_sample_polya": [vp, vp, vp, vp],
+            "cufe_ring_create": [C.POINTER(vp), i, i, vp, i],
+            "cufe_ring_destroy": [vp],
+            "cufe_ring_info": [vp, vp, vp, vp, vp],
+            "cufe_ntt_forward": [vp, vp, ll, vp],
+            "cufe_ntt_inverse": [vp, vp, ll, vp],
+            "cufe_dropin_configure": [i, i, i],
+            "cufe_dropin_status": [],
+            "rlwe_sife_setup_gpu": [vp, vp, vp, vp, vp],
+            "rlwe_sife_encrypt_gpu": [vp, vp, vp, vp, vp, i, vp],
+            "rlwe_sife_keygen_gpu": [vp, vp, vp, i, vp],
+            "rlwe_sife_decrypt_gmp_gpu": [vp, vp, vp, vp, i, vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None if name.startswith("rlwe_sife_") else C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != OK:
+        raise CufeError(rc, what)
+
+
+def _ptr(t):
+    """device or host address of a torch tensor / numpy array (None -> NULL)"""
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def _seeds(s):
+    if s is None:
+        return None
+    a = np.ascontiguousarray(np.asarray(s, dtype=np.uint8).reshape(-1))
+    return a
+
+
+def u32(t):
+    """torch int32 tensor -> numpy uint32 copy on the host"""
+    return t.detach().cpu().numpy().view(np.uint32)
+
+
+def _stream(stream, device):
+    """stream handle for a call: the given one, else torch's current stream on device"""
+    if stream is not None:
+        return stream
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream or None
+
+
+def _dev(shape, device):
+    import torch
+    return torch.empty(shape, dtype=torch.int32, device=device)
+
+
+def to_dev(a, device="cuda"):
+    import torch
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+    return torch.from_numpy(a.view(np.int32)).to(device)
+
+
+class Context:
+    """An IPFE parameter set (ring degree n, vector length l) on one device."""
+
+    def __init__(self, n, l, device=0):
+        L = lib()
+        self.n, self.l, self.device = n, l, device
+        h = C.c_void_p()
+        _check(L.cufe_create(C.byref(h), n, l, device), "cufe_create")
+        self.h = h
+        p = np.zeros(1, np.uint32)
+        dm = np.zeros(3, np.uint32)
+        _check(L.cufe_params(h, p.ctypes.data, dm.ctypes.data), "cufe_params")
+        self.p, self.delta_mod = int(p[0]), dm
+        self.dev = "cuda:%d" % device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cufe_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return lib().cufe_ctx_stream(self.h)
+
+    def sync(self, stream=None):
+        _check(lib().cufe_sync(self.h, _stream(stream, self.device)), "cufe_sync")
+
+    def tables(self):
+        psi = np.zeros((3, self.n), np.uint32)
+        ipsi = np.zeros((3, self.n), np.uint32)
+        _check(lib().cufe_tables(self.h, psi.ctypes.data, ipsi.ctypes.data), "cufe_tables")
+        return psi, ipsi
+
+    # ---- buffers
+    def mpk_buf(self):
+        return _dev((self.l + 1, 3, self.n), self.dev)
+
+    def msk_buf(self):
+        return _dev((self.l, 3, self.n), self.dev)
+
+    def ct_buf(self, batch):
+        return _dev((batch, self.l + 1, 3, self.n), self.dev)
+
+    # ---- scheme (device tensors; ordered on torch's current stream unless a stream is given)
+    def setup(self, seed_a, seed_s, seed_e, mpk=None, msk=None, stream=None):
+        mpk = self.mpk_buf() if mpk is None else mpk
+        msk = self.msk_buf() if msk is None else msk
+        sa, ss, se = _seeds(seed_a), _seeds(seed_s), _seeds(seed_e)
+        _check(lib().cufe_setup(self.h, _ptr(sa), _ptr(ss), _ptr(se), _ptr(mpk), _ptr(msk), _stream(stream, self.device)), "cufe_setup")
+        return mpk, msk
+
+    def setup_gpu_map(self, a_coeff, seed2, seed3, mpk=None, msk=None, stream=None):
+        import torch
+        mpk = self.mpk_buf() if mpk is None else mpk
+        msk = self.msk_buf() if msk is None else msk
+        mpk[self.l].copy_(torch.as_tensor(a_coeff).to(mpk.device).reshape(3, self.n))
+        s2, s3 = _seeds(seed2), _seeds(seed3)
+        _check(lib().cufe_setup_gpu_map(self.h, _ptr(s2), _ptr(s3), _ptr(mpk), _ptr(msk),
+                                         _stream(stream, self.device)), "cufe_setup_gpu_map")
+        return mpk, msk
+
+    def encrypt(self, x, mpk, seeds2, seeds3=None, ct=None, stream=None):
+        batch = x.shape[0]
+        ct = self.ct_buf(batch) if ct is None else ct
+        s2, s3 = _seeds(seeds2), _seeds(seeds3)
+        _check(lib().cufe_encrypt(self.h, batch, _ptr(x), _ptr(mpk), _ptr(s2), _ptr(s3), _ptr(ct), _stream(stream, self.device)),
+               "cufe_encrypt")
+        return ct
+
+    def encrypt_gpu_map(self, x, mpk, seed2, ct=None, stream=None):
+        batch = x.shape[0]
+        ct = self.ct_buf(batch) if ct is None else ct
+        s2 = _seeds(seed2)
+        _check(lib().cufe_encrypt_gpu_map(self.h, batch, _ptr(x), _ptr(mpk), _ptr(s2), _ptr(ct), _stream(stream, self.device)),
+               "cufe_encrypt_gpu_map")
+        return ct
+
+    def keygen(self, y, msk, y_signed=False, sky=None, stream=None):
+        nkeys = y.shape[0]
+        sky = _dev((nkeys, 3, self.n), self.dev) if sky is None else sky
+        _check(lib().cufe_keygen(self.h, nkeys, _ptr(y), int(y_signed), _ptr(msk), _ptr(sky), _stream(stream, self.device)), "cufe_keygen")
+        return sky
+
+    def decrypt(self, ct, y, sky, y_signed=False, dy=None, stream=None):
+        nct, nkeys = ct.shape[0], y.shape[0]
+        dy = _dev((nct, nkeys, 3, self.n), self.dev) if dy is None else dy
+        _check(lib().cufe_decrypt(self.h, nct, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(dy), _stream(stream, self.device)),
+               "cufe_decrypt")
+        return dy
+
+    def decode(self, dy, ncoeff=None, out=None, stream=None):
+        ncoeff = self.n if ncoeff is None else ncoeff
+        count = dy.numel() // (3 * self.n)
+        out = _dev((count, ncoeff), self.dev) if out is None else out
+        _check(lib().cufe_decode(self.h, count, _ptr(dy), ncoeff, _ptr(out), _stream(stream, self.device)), "cufe_decode")
+        return out
+
+    # ---- samplers
+    def sample_cpu_map(self, sig, keys, calls, nstreams=None, out=None, stream=None):
+        k = _seeds(keys)
+        ns = nstreams if nstreams is not None else (1 if k is None else len(k) // 32)
+        out = _dev((ns, calls, 3, self.n), self.dev) if out is None else out
+        _check(lib().cufe_sample_cpu_map(self.h, sig, ns, _ptr(k), calls, _ptr(out), _stream(stream, self.device)), "cufe_sample_cpu_map")
+        return out
+
+    def sample_gpu_map(self, sig, key, poly0, npolys, out=None, stream=None):
+        out = _dev((npolys, 3, self.n), self.dev) if out is None else out
+        k = _seeds(key)
+        _check(lib().cufe_sample_gpu_map(self.h, sig, _ptr(k), poly0, npolys, _ptr(out), _stream(stream, self.device)),
+               "cufe_sample_gpu_map")
+        return out
+
+    def sample_polya(self, seed, out=None, stream=None):
+        out = _dev((3, self.n), self.dev) if out is None else out
+        sd = _seeds(seed)
+        _check(lib().cufe_sample_polya(self.h, _ptr(sd), _ptr(out), _stream(stream, self.device)), "cufe_sample_polya")
+        return out
+
+
+class Ring:
+    """RNS ring for the negacyclic NTT kernels (k primes, degree n)."""
+
+    def __init__(self, n, k, primes=None, device=0):
+        L = lib()
+        self.n, self.k, self.device = n, k, device
+        h = C.c_void_p()
+        pr = None if primes is None else np.ascontiguousarray(primes, np.uint32)
+        _check(L.cufe_ring_create(C.byref(h), n, k, _ptr(pr), device), "cufe_ring_create")
+        self.h = h
+        self.primes = np.zeros(k, np.uint32)
+        self.roots = np.zeros(k, np.uint32)
+        self.psi = np.zeros((k, n), np.uint32)
+        self.psi_inv = np.zeros((k, n), np.uint32)
+        _check(L.cufe_ring_info(h, self.primes.ctypes.data, self.roots.ctypes.data, self.psi.ctypes.data,
+                                self.psi_inv.ctypes.data), "cufe_ring_info")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cufe_ring_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, data, stream=None):
+        npoly = data.numel() // (self.k * self.n)
+        _check(lib().cufe_ntt_forward(self.h, _ptr(data), npoly, _stream(stream, self.device)), "cufe_ntt_forward")
+        return data
+
+    def inverse(self, data, stream=None):
+        npoly = data.numel() // (self.k * self.n)
+        _check(lib().cufe_ntt_inverse(self.h, _ptr(data), npoly, _stream(stream, self.device)), "cufe_ntt_inverse")
+        return data

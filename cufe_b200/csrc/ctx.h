@@ -1,0 +1,76 @@
+// ctx.h -- host-side objects behind the C ABI: RNS rings and IPFE contexts.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cufe_internal.cuh"
+
+namespace cufe {
+
+typedef unsigned __int128 u128;
+
+// An RNS ring Z_q[X]/(X^n + 1) with device twiddle tables.
+struct Ring {
+  int device = 0, n = 0, logn = 0, k = 0;
+  std::vector<uint32_t> q, psi_root;       // primes and the primitive 2n-th roots used
+  std::vector<uint32_t> h_psi, h_ipsi;     // host copies [k][n] (bit-reversed powers)
+  uint32_t *d_tab = nullptr;               // psi, psi_sh, ipsi, ipsi_sh: 4 x [k][n]
+  RingArgs args{};
+  int init(int n, int k, const uint32_t *primes, int device);
+  void release();
+};
+
+// Primes q < 2^31 with q = 1 mod 2^14 (NTT-friendly for every n <= 8192): the params.h
+// primes first, then the largest others.
+std::vector<uint32_t> ntt_primes(int k);
+
+struct Ctx {
+  int device = 0, n = 0, l = 0, num_sms = 148;
+  Ring ring;  // k = 3 params.h primes
+  cudaStream_t stream = nullptr;
+  // scheme constants (src/params.h:14-28 recomputed for this l)
+  uint32_t p = 0;
+  u128 q = 0, qhalf = 0;
+  uint32_t delta_mod[3]{}, delta_sh[3]{};
+  uint32_t crt_c1 = 0, crt_c1_sh = 0, crt_c2 = 0, crt_c2_sh = 0;
+  // workspace
+  uint8_t *ws = nullptr;
+  size_t ws_bytes = 0;
+  uint32_t *d_status = nullptr;  // sampler status word (device)
+  std::mutex mu;                 // serialises host calls on this context
+
+  int init(int n, int l, int device);
+  void release();
+  int ensure_ws(size_t bytes);
+  // NULL selects the legacy default stream, as everywhere in CUDA
+  cudaStream_t pick(void *s) const { return static_cast<cudaStream_t>(s); }
+  int check_status(cudaStream_t s);  // synchronises s and reports the sampler status word
+};
+
+int ntt_launch(const RingArgs &ra, uint32_t *data, long long nres, bool inverse, cudaStream_t s);
+int ntt_fwd_shoup_launch(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s);
+
+int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,
+                      uint32_t *d_msk, cudaStream_t s);
+int ctx_setup_gpu_map(Ctx &c, const uint8_t *seed2, const uint8_t *seed3, uint32_t *d_mpk, uint32_t *d_msk,
+                      cudaStream_t s);
+int ctx_encrypt_cpu_map(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                        const uint8_t *seeds3, uint32_t *d_ct, cudaStream_t s);
+int ctx_encrypt_gpu_map(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seed2,
+                        uint32_t *d_ct, cudaStream_t s);
+int ctx_keygen(Ctx &c, int nkeys, const uint32_t *d_y, int y_signed, const uint32_t *d_msk, uint32_t *d_sky,
+               cudaStream_t s);
+int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s);
+int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s);
+int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
+                       cudaStream_t s);
+int ctx_sample_gpu_map(Ctx &c, int sig, const uint8_t *key, int poly0, int npolys, uint32_t *d_out,
+                       cudaStream_t s);
+int ctx_sample_polya(Ctx &c, const uint8_t *seed, uint32_t *d_a, cudaStream_t s);
+
+}  // namespace cufe

@@ -1,0 +1,863 @@
+// ipfe.cu -- RNS rings, NTT launchers and the RLWE-IPFE scheme kernels (setup, encrypt,
+// keygen, decrypt, decode) with their host orchestration.
+//
+// Scheme (reference: src/rlwe_sife.c, src/rlwe_sife_gpu.cu): ring Z_q[X]/(X^n+1), q = q0 q1 q2
+// in RNS; mpk_i = a*s_i + e_i (NTT domain), c_l = INTT(a^ r^) + f_0,
+// c_i = INTT(pk_i^ r^) + f_i + floor(q/p) x_i, sk_y = sum y_i s_i,
+// d_y = sum y_i c_i - c_l * sk_y, decoded as round(p d_y / q).
+#include <algorithm>
+#include <cstring>
+
+#include "ctx.h"
+#include "ntt.cuh"
+#include "sampler_host.h"
+
+namespace cufe {
+
+// ================================================================== host number theory
+
+static uint64_t powmod(uint64_t b, uint64_t e, uint64_t q) {
+  uint64_t r = 1 % q;
+  b %= q;
+  while (e) {
+    if (e & 1) r = r * b % q;
+    b = b * b % q;
+    e >>= 1;
+  }
+  return r;
+}
+static uint64_t invmod(uint64_t a, uint64_t q) { return powmod(a, q - 2, q); }
+
+static bool is_prime32(uint32_t n) {  // deterministic Miller-Rabin for n < 3.2e9
+  if (n < 2) return false;
+  for (uint32_t p : {2u, 3u, 5u, 7u})
+    if (n % p == 0) return n == p;
+  uint64_t d = n - 1;
+  int s = 0;
+  while (!(d & 1)) d >>= 1, ++s;
+  for (uint64_t a : {2ull, 3ull, 5ull, 7ull}) {
+    uint64_t x = powmod(a, d, n);
+    if (x == 1 || x == n - 1) continue;
+    bool comp = true;
+    for (int r = 1; r < s; ++r) {
+      x = x * x % n;
+      if (x == n - 1) {
+        comp = false;
+        break;
+      }
+    }
+    if (comp) return false;
+  }
+  return true;
+}
+
+static uint32_t primitive_root(uint32_t q) {
+  std::vector<uint64_t> f;
+  uint64_t m = q - 1;
+  for (uint64_t p = 2; p * p <= m; ++p)
+    if (m % p == 0) {
+      f.push_back(p);
+      while (m % p == 0) m /= p;
+    }
+  if (m > 1) f.push_back(m);
+  for (uint32_t g = 2;; ++g) {
+    bool ok = true;
+    for (uint64_t p : f)
+      if (powmod(g, (q - 1) / p, q) == 1) {
+        ok = false;
+        break;
+      }
+    if (ok) return g;
+  }
+}
+
+// psi_j: primitive 8192-th roots of unity of the reference twiddle tables
+// (src/consts.h: psi[j][k] = psi_j^{bitrev12(k)}, i.e. psi_j = psi[j][2048]).
+static const uint32_t kPsi8192[3] = {3689u, 1689795u, 456478u};
+
+static uint32_t root_for(uint32_t q, int n) {
+  for (int j = 0; j < 3; ++j) {
+    if (q != kRefPrimes[j]) continue;
+    if (2 * n <= 8192) return (uint32_t)powmod(kPsi8192[j], 8192 / (2 * n), q);
+    // n = 8192: the smaller square root of psi_8192 (same chain of tables)
+    const uint64_t h = powmod(primitive_root(q), (q - 1) / 16384, q);
+    uint64_t best = 0;
+    for (uint64_t t = 1; t < 16384; t += 2) {
+      const uint64_t c = powmod(h, t, q);
+      if (c * c % q == kPsi8192[j] && (best == 0 || c < best)) best = c;
+    }
+    return (uint32_t)best;
+  }
+  return (uint32_t)powmod(primitive_root(q), (q - 1) / (2ull * n), q);
+}
+
+std::vector<uint32_t> ntt_primes(int k) {
+  std::vector<uint32_t> v;
+  for (int j = 0; j < 3 && (int)v.size() < k; ++j) v.push_back(kRefPrimes[j]);
+  for (uint64_t c = ((1ull << 31) - 1) / 16384 * 16384 + 1; (int)v.size() < k; c -= 16384) {
+    const uint32_t cc = (uint32_t)c;
+    if (std::find(v.begin(), v.end(), cc) == v.end() && is_prime32(cc)) v.push_back(cc);
+  }
+  return v;
+}
+
+static unsigned bitrev(unsigned x, int bits) {
+  unsigned r = 0;
+  for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+
+int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
+  if (n_ < 16 || n_ > 8192 || (n_ & (n_ - 1)) || k_ < 1 || k_ > kMaxModuli) return CUFE_ERR_INVALID;
+  n = n_;
+  k = k_;
+  device = dev;
+  logn = 0;
+  while ((1 << logn) < n) ++logn;
+  q = primes ? std::vector<uint32_t>(primes, primes + k) : ntt_primes(k);
+  for (uint32_t qq : q)
+    if (qq >= (1u << 31) || (qq - 1) % (2u * n) != 0 || !is_prime32(qq)) return CUFE_ERR_INVALID;
+  std::vector<uint32_t> tab(4 * (size_t)k * n);
+  h_psi.assign((size_t)k * n, 0);
+  h_ipsi.assign((size_t)k * n, 0);
+  psi_root.assign(k, 0);
+  std::memset(&args, 0, sizeof(args));
+  std::vector<uint64_t> pw(n), ipw(n);
+  for (int m = 0; m < k; ++m) {
+    const uint64_t qq = q[m], w = root_for(q[m], n), wi = invmod(w, qq);
+    psi_root[m] = (uint32_t)w;
+    pw[0] = ipw[0] = 1;
+    for (int e = 1; e < n; ++e) pw[e] = pw[e - 1] * w % qq, ipw[e] = ipw[e - 1] * wi % qq;
+    for (int i = 0; i < n; ++i) {
+      const uint32_t a = (uint32_t)pw[bitrev(i, logn)], b = (uint32_t)ipw[bitrev(i, logn)];
+      h_psi[(size_t)m * n + i] = a;
+      h_ipsi[(size_t)m * n + i] = b;
+      tab[(size_t)(0 * k + m) * n + i] = a;
+      tab[(size_t)(1 * k + m) * n + i] = shoup_of(a, (uint32_t)qq);
+      tab[(size_t)(2 * k + m) * n + i] = b;
+      tab[(size_t)(3 * k + m) * n + i] = shoup_of(b, (uint32_t)qq);
+    }
+    args.q[m] = (uint32_t)qq;
+    args.ninv[m] = (uint32_t)invmod(n, qq);
+    args.ninv_sh[m] = shoup_of(args.ninv[m], (uint32_t)qq);
+    args.w1n[m] = (uint32_t)((uint64_t)h_ipsi[(size_t)m * n + 1] * args.ninv[m] % qq);
+    args.w1n_sh[m] = shoup_of(args.w1n[m], (uint32_t)qq);
+  }
+  args.n = n;
+  args.logn = logn;
+  args.k = k;
+  CUFE_CUDA(cudaSetDevice(device));
+  CUFE_CUDA(cudaMalloc(&d_tab, tab.size() * 4));
+  CUFE_CUDA(cudaMemcpy(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice));
+  args.psi = d_tab;
+  args.psi_sh = d_tab + (size_t)k * n;
+  args.ipsi = d_tab + 2 * (size_t)k * n;
+  args.ipsi_sh = d_tab + 3 * (size_t)k * n;
+  return CUFE_OK;
+}
+
+void Ring::release() {
+  if (d_tab) cudaFree(d_tab);
+  d_tab = nullptr;
+}
+
+// ================================================================== NTT kernels
+
+namespace {
+
+template <int LOGN>
+constexpr int ppc() {  // residue polynomials per CTA (>= 256 threads per CTA)
+  return NttPlan<LOGN>::T >= 256 ? 1 : 256 / NttPlan<LOGN>::T;
+}
+
+__device__ __forceinline__ void load16(const uint32_t *p, uint32_t (&a)[16]) {
+  const uint4 *v = reinterpret_cast<const uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint4 t = v[i];
+    a[4 * i] = t.x;
+    a[4 * i + 1] = t.y;
+    a[4 * i + 2] = t.z;
+    a[4 * i + 3] = t.w;
+  }
+}
+__device__ __forceinline__ void store16(uint32_t *p, const uint32_t (&a)[16]) {
+  uint4 *v = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = make_uint4(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]);
+}
+
+// MODE 0 forward, 1 forward + Shoup companions into sh, 2 inverse
+template <int LOGN, int MODE>
+__global__ void __launch_bounds__(512) k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long nres,
+                                             RingArgs ra) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x;
+  const long long r = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool act = r < nres;
+  const long long rr = act ? r : nres - 1;
+  const int m = (int)(rr % ra.k);
+  const uint32_t q = ra.q[m];
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t *d = data + rr * P::N;
+  uint32_t a[16];
+  if (MODE != 2) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) a[e] = d[P::template idx<0>(th, e)];
+    ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi + (size_t)m * P::N, ra.psi_sh + (size_t)m * P::N);
+    if (act) {
+      store16(d + th * 16, a);
+      if (MODE == 1) {
+        uint32_t b[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) b[e] = (uint32_t)(((uint64_t)a[e] << 32) / q);
+        store16(sh + rr * P::N + th * 16, b);
+      }
+    }
+  } else {
+    load16(d + th * 16, a);
+    ntt_inv_core<LOGN>(a, sm, th, q, ra.ipsi + (size_t)m * P::N, ra.ipsi_sh + (size_t)m * P::N, ra.ninv[m],
+                       ra.ninv_sh[m], ra.w1n[m], ra.w1n_sh[m]);
+    if (act) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) d[P::template idx<0>(th, e)] = a[e];
+    }
+  }
+}
+
+template <int LOGN, int MODE>
+int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
+  using P = NttPlan<LOGN>;
+  constexpr int G = ppc<LOGN>();
+  const size_t smem = (size_t)G * P::N * 4;
+  static bool attr = false;
+  if (!attr) {
+    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    attr = true;
+  }
+  const long long grid = (nres + G - 1) / G;
+  if (grid <= 0) return CUFE_OK;
+  k_ntt<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+template <int MODE>
+int launch_ntt(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
+  switch (ra.logn) {
+    case 4: return launch_ntt_t<4, MODE>(ra, data, sh, nres, s);
+    case 5: return launch_ntt_t<5, MODE>(ra, data, sh, nres, s);
+    case 6: return launch_ntt_t<6, MODE>(ra, data, sh, nres, s);
+    case 7: return launch_ntt_t<7, MODE>(ra, data, sh, nres, s);
+    case 8: return launch_ntt_t<8, MODE>(ra, data, sh, nres, s);
+    case 9: return launch_ntt_t<9, MODE>(ra, data, sh, nres, s);
+    case 10: return launch_ntt_t<10, MODE>(ra, data, sh, nres, s);
+    case 11: return launch_ntt_t<11, MODE>(ra, data, sh, nres, s);
+    case 12: return launch_ntt_t<12, MODE>(ra, data, sh, nres, s);
+    case 13: return launch_ntt_t<13, MODE>(ra, data, sh, nres, s);
+  }
+  return CUFE_ERR_INVALID;
+}
+
+// ================================================================== scheme kernels
+
+struct SchemeArgs {
+  RingArgs ra;
+  int l;
+  uint32_t delta_mod[3], delta_sh[3];
+  uint64_t mu[3];
+};
+
+__device__ __forceinline__ uint32_t y_residue(uint32_t y, int y_signed, uint32_t q, uint64_t mu) {
+  if (!y_signed) return mod_u64(y, mu, q);
+  const int32_t ys = (int32_t)y;
+  if (ys >= 0) return mod_u64((uint64_t)ys, mu, q);
+  const uint32_t r = mod_u64((uint64_t)(-(int64_t)ys), mu, q);
+  return r ? q - r : 0u;
+}
+
+// mpk_i = a^ * NTT(s_i) + e^_i for residue polynomials r = 3i + m (src/rlwe_sife.c:69-76)
+template <int LOGN>
+__global__ void __launch_bounds__(512) k_setup_mpk(const uint32_t *__restrict__ msk, const uint32_t *__restrict__ ehat,
+                                                   const uint32_t *__restrict__ ahat,
+                                                   const uint32_t *__restrict__ ahat_sh, uint32_t *__restrict__ mpk,
+                                                   long long nres, RingArgs ra) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x;
+  const long long r = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool act = r < nres;
+  const long long rr = act ? r : nres - 1;
+  const int m = (int)(rr % 3);
+  const uint32_t q = ra.q[m];
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t a[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = msk[rr * P::N + P::template idx<0>(th, e)];
+  ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi + (size_t)m * P::N, ra.psi_sh + (size_t)m * P::N);
+  uint32_t w[16], wsh[16], ev[16];
+  load16(ahat + (size_t)m * P::N + th * 16, w);
+  load16(ahat_sh + (size_t)m * P::N + th * 16, wsh);
+  load16(ehat + rr * P::N + th * 16, ev);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = mod_add(shoup_mul(a[e], w[e], wsh[e], q), ev[e], q);
+  if (act) store16(mpk + rr * P::N + th * 16, a);
+}
+
+// Fused encryption (src/rlwe_sife.c:157-176): for instance b and residue polynomial
+// r = 3i + m of the ciphertext, c = INTT(pk_r * r^) + f + floor(q/p) x_i.  CTAs are ordered
+// residue-major so the instances of one pk polynomial run together (pk read once per batch).
+template <int LOGN>
+__global__ void __launch_bounds__(512)
+    k_encrypt(const uint32_t *__restrict__ mpk, const uint32_t *__restrict__ rhat, const uint32_t *__restrict__ rhat_sh,
+              long long rhat_stride, const uint32_t *__restrict__ f3, long long f3_stride,
+              const uint32_t *__restrict__ f0, long long f0_stride, const uint32_t *__restrict__ x,
+              uint32_t *__restrict__ ct, int batch, long long nwork, SchemeArgs sa) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x;
+  const long long wi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool act = wi < nwork;
+  const long long ww = act ? wi : nwork - 1;
+  const int l = sa.l;
+  const long long res = ww / batch;
+  const int b = (int)(ww - res * batch);
+  const int m = (int)(res % 3), i = (int)(res / 3);
+  const uint32_t q = sa.ra.q[m];
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t a[16], w[16], wsh[16];
+  load16(mpk + res * P::N + th * 16, a);
+  load16(rhat + b * rhat_stride + (size_t)m * P::N + th * 16, w);
+  load16(rhat_sh + b * rhat_stride + (size_t)m * P::N + th * 16, wsh);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
+  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi + (size_t)m * P::N, sa.ra.ipsi_sh + (size_t)m * P::N, sa.ra.ninv[m],
+                     sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
+  const uint32_t *f;
+  uint32_t msg = 0;
+  if (i < l) {
+    f = f3 + b * f3_stride + ((size_t)i * 3 + m) * P::N;
+    const uint32_t xr = mod_u64(x[(size_t)b * l + i], sa.mu[m], q);
+    msg = shoup_mul(xr, sa.delta_mod[m], sa.delta_sh[m], q);
+  } else {
+    f = f0 + b * f0_stride + (size_t)m * P::N;
+  }
+  uint32_t *c = ct + ((size_t)b * (l + 1) * 3 + res) * P::N;
+  if (act) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const int j = P::template idx<0>(th, e);
+      c[j] = mod_add(mod_add(a[e], f[j], q), msg, q);
+    }
+  }
+}
+
+// sk_y = sum_i (y_i mod q_m) msk_i (src/rlwe_sife.c:215-245); KCH keys per pass over msk
+template <int KCH>
+__global__ void __launch_bounds__(256) k_keygen(const uint32_t *__restrict__ y, int y_signed, int nkeys,
+                                                const uint32_t *__restrict__ msk, uint32_t *__restrict__ sky, int n,
+                                                SchemeArgs sa) {
+  extern __shared__ uint32_t smem_u32[];
+  const int l = sa.l, m = blockIdx.y, k0 = blockIdx.z * KCH;
+  const uint32_t q = sa.ra.q[m];
+  uint32_t *yq = smem_u32, *ys = smem_u32 + KCH * l;
+  for (int t = threadIdx.x; t < KCH * l; t += blockDim.x) {
+    const int kk = t / l, i = t - kk * l;
+    uint32_t v = 0;
+    if (k0 + kk < nkeys) v = y_residue(y[(size_t)(k0 + kk) * l + i], y_signed, q, sa.mu[m]);
+    yq[t] = v;
+    ys[t] = (uint32_t)(((uint64_t)v << 32) / q);
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint64_t acc[KCH];
+#pragma unroll
+  for (int kk = 0; kk < KCH; ++kk) acc[kk] = 0;
+  for (int i = 0; i < l; ++i) {
+    const uint32_t v = __ldg(msk + ((size_t)i * 3 + m) * n + j);
+#pragma unroll
+    for (int kk = 0; kk < KCH; ++kk) acc[kk] += shoup_lazy(v, yq[kk * l + i], ys[kk * l + i], q);
+  }
+#pragma unroll
+  for (int kk = 0; kk < KCH; ++kk)
+    if (k0 + kk < nkeys) sky[((size_t)(k0 + kk) * 3 + m) * n + j] = mod_u64(acc[kk], sa.mu[m], q);
+}
+
+// d_y for ciphertext c and key k, residue m (src/rlwe_sife.c:248-278):
+// sum_i y_i c_i - INTT(NTT(c_l) NTT(sk_y)); one residue polynomial per thread group.
+template <int LOGN>
+__global__ void __launch_bounds__(512)
+    k_decrypt(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ clhat, const uint32_t *__restrict__ skhat,
+              const uint32_t *__restrict__ skhat_sh, const uint32_t *__restrict__ y, int y_signed, int nct, int nkeys,
+              uint32_t *__restrict__ dy, long long nwork, SchemeArgs sa) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x, l = sa.l;
+  const long long wi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool act = wi < nwork;
+  const long long ww = act ? wi : nwork - 1;
+  // work index = (c * nkeys + k) * 3 + m
+  const int m = (int)(ww % 3);
+  const long long ck = ww / 3;
+  const int key = (int)(ck % nkeys), c = (int)(ck / nkeys);
+  const uint32_t q = sa.ra.q[m];
+  uint32_t *sm = smem_u32 + threadIdx.y * (P::N + 2 * l);
+  uint32_t *yq = sm + P::N, *ys = yq + l;
+  for (int i = th; i < l; i += P::T) {
+    const uint32_t v = y_residue(y[(size_t)key * l + i], y_signed, q, sa.mu[m]);
+    yq[i] = v;
+    ys[i] = (uint32_t)(((uint64_t)v << 32) / q);
+  }
+  uint32_t a[16], w[16], wsh[16];
+  load16(clhat + ((size_t)c * 3 + m) * P::N + th * 16, a);
+  load16(skhat + ((size_t)key * 3 + m) * P::N + th * 16, w);
+  load16(skhat_sh + ((size_t)key * 3 + m) * P::N + th * 16, wsh);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
+  __syncthreads();
+  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi + (size_t)m * P::N, sa.ra.ipsi_sh + (size_t)m * P::N, sa.ra.ninv[m],
+                     sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
+  uint64_t acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = 0;
+  const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * P::N + (size_t)m * P::N;
+  for (int i = 0; i < l; ++i) {
+    const uint32_t yv = yq[i], yh = ys[i];
+    const uint32_t *ci = cb + (size_t)i * 3 * P::N;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] += shoup_lazy(__ldg(ci + P::template idx<0>(th, e)), yv, yh, q);
+  }
+  if (act) {
+    uint32_t *o = dy + ww * P::N;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) o[P::template idx<0>(th, e)] = mod_sub(mod_u64(acc[e], sa.mu[m], q), a[e], q);
+  }
+}
+
+struct DecodeArgs {
+  uint32_t q0, q1, q2;
+  uint32_t c1, c1_sh, c2, c2_sh;
+  uint64_t mu2;
+  uint64_t q01;
+  unsigned long long qlo, qhi, hlo, hhi;  // q and floor(q/2) as 128-bit halves
+  uint32_t p;
+  int n;
+};
+
+// crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332): Garner
+// to x in [0, q), then floor(p x / q) + (remainder > floor(q/2)).
+__global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff, uint32_t *__restrict__ out,
+                         DecodeArgs d) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)count * ncoeff) return;
+  const int cnt = (int)(gid / ncoeff), k = (int)(gid - (long long)cnt * ncoeff);
+  const uint32_t *v = dy + (size_t)cnt * 3 * d.n + k;
+  const uint32_t v0 = v[0], v1 = v[d.n], v2 = v[2 * (size_t)d.n];
+  const uint32_t t1 = mod_red1(v1 + d.q1 - v0 % d.q1, d.q1);
+  const uint32_t u1 = shoup_mul(t1, d.c1, d.c1_sh, d.q1);
+  const uint64_t x1 = (uint64_t)v0 + (uint64_t)d.q0 * u1;
+  const uint32_t xm = mod_u64(x1, d.mu2, d.q2);
+  const uint32_t t2 = mod_red1(v2 + d.q2 - xm, d.q2);
+  const uint32_t u2 = shoup_mul(t2, d.c2, d.c2_sh, d.q2);
+  const u128 Q = ((u128)d.qhi << 64) | d.qlo, H = ((u128)d.hhi << 64) | d.hlo;
+  const u128 x = (u128)x1 + (u128)d.q01 * u2;
+  const u128 a = x * d.p;
+  // quotient < p + 1: estimate in double, correct exactly
+  long long qe = (long long)floor((double)x / (double)Q * (double)d.p);
+  if (qe < 0) qe = 0;
+  u128 prod = (u128)qe * Q;
+  while (prod > a) {
+    --qe;
+    prod -= Q;
+  }
+  u128 rem = a - prod;
+  while (rem >= Q) {
+    ++qe;
+    rem -= Q;
+  }
+  if (rem > H) ++qe;
+  out[gid] = (uint32_t)qe;
+}
+
+}  // namespace
+
+int ntt_launch(const RingArgs &ra, uint32_t *data, long long nres, bool inverse, cudaStream_t s) {
+  return inverse ? launch_ntt<2>(ra, data, nullptr, nres, s) : launch_ntt<0>(ra, data, nullptr, nres, s);
+}
+int ntt_fwd_shoup_launch(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
+  return launch_ntt<1>(ra, data, sh, nres, s);
+}
+
+// ================================================================== context
+
+int Ctx::init(int n_, int l_, int dev) {
+  if (l_ < 1 || l_ > 65536) return CUFE_ERR_INVALID;
+  n = n_;
+  l = l_;
+  device = dev;
+  int rc = ring.init(n_, 3, kRefPrimes, dev);
+  if (rc) return rc;
+  CUFE_CUDA(cudaSetDevice(device));
+  CUFE_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  CUFE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CUFE_CUDA(cudaMalloc(&d_status, 256));
+  CUFE_CUDA(cudaMemset(d_status, 0, 256));
+  rc = sampler_init_device();
+  if (rc) return rc;
+  p = 4u * 16u * (uint32_t)l + 1u;  // B_x * B_y * l + 1 (src/params.h:26)
+  q = (u128)kRefPrimes[0] * kRefPrimes[1] * kRefPrimes[2];
+  qhalf = q / 2;
+  const u128 delta = q / p;  // floor(q/p) (src/params.h:27)
+  for (int j = 0; j < 3; ++j) {
+    delta_mod[j] = (uint32_t)(delta % kRefPrimes[j]);
+    delta_sh[j] = shoup_of(delta_mod[j], kRefPrimes[j]);
+  }
+  crt_c1 = (uint32_t)invmod(kRefPrimes[0], kRefPrimes[1]);
+  crt_c2 = (uint32_t)invmod((uint64_t)kRefPrimes[0] * kRefPrimes[1] % kRefPrimes[2], kRefPrimes[2]);
+  crt_c1_sh = shoup_of(crt_c1, kRefPrimes[1]);
+  crt_c2_sh = shoup_of(crt_c2, kRefPrimes[2]);
+  return CUFE_OK;
+}
+
+void Ctx::release() {
+  if (ws) cudaFree(ws);
+  if (d_status) cudaFree(d_status);
+  if (stream) cudaStreamDestroy(stream);
+  ring.release();
+  ws = nullptr;
+  d_status = nullptr;
+  stream = nullptr;
+}
+
+int Ctx::ensure_ws(size_t bytes) {
+  if (bytes <= ws_bytes) return CUFE_OK;
+  CUFE_CUDA(cudaDeviceSynchronize());
+  if (ws) CUFE_CUDA(cudaFree(ws));
+  ws = nullptr;
+  ws_bytes = 0;
+  const size_t want = bytes + (bytes >> 3);
+  if (cudaMalloc(&ws, want) != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error("workspace allocation of " + std::to_string(want) + " bytes failed");
+    return CUFE_ERR_NOMEM;
+  }
+  ws_bytes = want;
+  return CUFE_OK;
+}
+
+int Ctx::check_status(cudaStream_t s) {
+  uint32_t st = 0;
+  CUFE_CUDA(cudaMemcpyAsync(&st, d_status, 4, cudaMemcpyDeviceToHost, s));
+  CUFE_CUDA(cudaStreamSynchronize(s));
+  if (st) {
+    CUFE_CUDA(cudaMemsetAsync(d_status, 0, 4, s));
+    set_last_error(std::string("sampler status ") + std::to_string(st) +
+                   ((st & 2) ? " (refill range exhausted)" : " (uniform draw beyond the refill buffer)"));
+    return CUFE_ERR_SAMPLER;
+  }
+  return CUFE_OK;
+}
+
+static SchemeArgs scheme_args(const Ctx &c) {
+  SchemeArgs sa;
+  sa.ra = c.ring.args;
+  sa.l = c.l;
+  for (int j = 0; j < 3; ++j) {
+    sa.delta_mod[j] = c.delta_mod[j];
+    sa.delta_sh[j] = c.delta_sh[j];
+    sa.mu[j] = (uint64_t)(((u128)1 << 64) / kRefPrimes[j]);
+  }
+  return sa;
+}
+
+struct Arena {
+  uint8_t *p;
+  size_t used = 0;
+  explicit Arena(uint8_t *base) : p(base) {}
+  template <class T>
+  T *take(size_t count) {
+    T *r = reinterpret_cast<T *>(p + used);
+    used += (count * sizeof(T) + 255) & ~(size_t)255;
+    return r;
+  }
+};
+
+static std::vector<uint32_t> expand_keys(int count, const uint8_t *keys) {
+  std::vector<uint32_t> rk((size_t)count * 60, 0u);  // null keys: all-zero schedule
+  if (keys)
+    for (int i = 0; i < count; ++i) aes_key_expand(keys + 32 * (size_t)i, rk.data() + 60 * (size_t)i);
+  return rk;
+}
+
+template <class F>
+static int dispatch_logn(int logn, F &&f) {
+  switch (logn) {
+    case 4: return f(std::integral_constant<int, 4>());
+    case 5: return f(std::integral_constant<int, 5>());
+    case 6: return f(std::integral_constant<int, 6>());
+    case 7: return f(std::integral_constant<int, 7>());
+    case 8: return f(std::integral_constant<int, 8>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 10: return f(std::integral_constant<int, 10>());
+    case 11: return f(std::integral_constant<int, 11>());
+    case 12: return f(std::integral_constant<int, 12>());
+    case 13: return f(std::integral_constant<int, 13>());
+  }
+  return CUFE_ERR_INVALID;
+}
+
+// shared tail of both setups: a^ = NTT(a) in place, e^ = NTT(e), mpk_i = a^ NTT(s_i) + e^_i
+static int setup_tail(Ctx &c, uint32_t *d_mpk, const uint32_t *d_msk, uint32_t *e, uint32_t *a_sh, cudaStream_t s) {
+  const int n = c.n, l = c.l;
+  uint32_t *ahat = d_mpk + (size_t)l * 3 * n;
+  int rc = ntt_fwd_shoup_launch(c.ring.args, ahat, a_sh, 3, s);
+  if (rc) return rc;
+  rc = ntt_launch(c.ring.args, e, (long long)l * 3, false, s);
+  if (rc) return rc;
+  const long long nres = (long long)l * 3;
+  return dispatch_logn(c.ring.logn, [&](auto L) {
+    constexpr int LOGN = decltype(L)::value;
+    constexpr int G = ppc<LOGN>();
+    CUFE_CUDA(cudaFuncSetAttribute(k_setup_mpk<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+        d_msk, e, ahat, a_sh, d_mpk, nres, c.ring.args);
+    CUFE_CUDA(cudaGetLastError());
+    return CUFE_OK;
+  });
+}
+
+int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,
+                      uint32_t *d_msk, cudaStream_t s) {
+  const int n = c.n, l = c.l;
+  const size_t poly = (size_t)3 * n;
+  const size_t samp_ws = cpu_map_workspace_bytes(2, l, n, 0);
+  int rc = c.ensure_ws(samp_ws + (2 * l + 2) * poly * 4 + 4096 + 4 * 60 * 4);
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *rk = ar.take<uint32_t>(3 * 60);
+  uint32_t *se = ar.take<uint32_t>(2 * (size_t)l * poly);  // [2][l][3][n]: s, e
+  uint32_t *a_sh = ar.take<uint32_t>(poly);
+  void *sws = ar.take<uint8_t>(samp_ws);
+  std::vector<uint32_t> keys(3 * 60, 0u);
+  aes_key_expand(seed_a, keys.data());
+  if (seed_s) aes_key_expand(seed_s, keys.data() + 60);
+  aes_key_expand(seed_e, keys.data() + 120);
+  CUFE_CUDA(cudaMemcpyAsync(rk, keys.data(), keys.size() * 4, cudaMemcpyHostToDevice, s));
+  rc = sample_polya(rk, n, d_mpk + (size_t)l * poly, s);
+  if (rc) return rc;
+  rc = sample_cpu_map(0, 2, rk + 60, l, n, se, sws, c.d_status, c.num_sms, s);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMemcpyAsync(d_msk, se, (size_t)l * poly * 4, cudaMemcpyDeviceToDevice, s));
+  return setup_tail(c, d_mpk, d_msk, se + (size_t)l * poly, a_sh, s);
+}
+
+int ctx_setup_gpu_map(Ctx &c, const uint8_t *seed2, const uint8_t *seed3, uint32_t *d_mpk, uint32_t *d_msk,
+                      cudaStream_t s) {
+  const int n = c.n, l = c.l;
+  const size_t poly = (size_t)3 * n;
+  int rc = c.ensure_ws((size_t)(l + 1) * poly * 4 + 4096 + 2 * 60 * 4);
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *rk = ar.take<uint32_t>(2 * 60);
+  uint32_t *e = ar.take<uint32_t>((size_t)l * poly);
+  uint32_t *a_sh = ar.take<uint32_t>(poly);
+  std::vector<uint32_t> keys(2 * 60, 0u);
+  aes_key_expand(seed2, keys.data());
+  aes_key_expand(seed3, keys.data() + 60);
+  CUFE_CUDA(cudaMemcpyAsync(rk, keys.data(), keys.size() * 4, cudaMemcpyHostToDevice, s));
+  rc = sample_gpu_map(0, rk, 0, l, n, d_msk, c.d_status, s);
+  if (rc) return rc;
+  rc = sample_gpu_map(0, rk + 60, 0, l, n, e, c.d_status, s);
+  if (rc) return rc;
+  return setup_tail(c, d_mpk, d_msk, e, a_sh, s);
+}
+
+static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint32_t *rhat,
+                        const uint32_t *rhat_sh, long long rhat_stride, const uint32_t *f3, long long f3_stride,
+                        const uint32_t *f0, long long f0_stride, uint32_t *d_ct, cudaStream_t s) {
+  const long long nwork = (long long)(c.l + 1) * 3 * batch;
+  const SchemeArgs sa = scheme_args(c);
+  return dispatch_logn(c.ring.logn, [&](auto L) {
+    constexpr int LOGN = decltype(L)::value;
+    constexpr int G = ppc<LOGN>();
+    CUFE_CUDA(cudaFuncSetAttribute(k_encrypt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    k_encrypt<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+        d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
+    CUFE_CUDA(cudaGetLastError());
+    return CUFE_OK;
+  });
+}
+
+size_t encrypt_workspace_bytes(int n, int l, int batch) {
+  const size_t poly = (size_t)3 * n;
+  return cpu_map_workspace_bytes(batch, l, n, 2) + cpu_map_workspace_bytes(batch, 2, n, 1) +
+         (size_t)batch * ((size_t)l * poly + 2 * poly + 2 * poly) * 4 + (size_t)batch * 2 * 60 * 4 + 16 * 256;
+}
+
+int ctx_encrypt_cpu_map(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                        const uint8_t *seeds3, uint32_t *d_ct, cudaStream_t s) {
+  if (batch < 1 || !seeds2) return CUFE_ERR_INVALID;
+  const int n = c.n, l = c.l;
+  const size_t poly = (size_t)3 * n;
+  const size_t ws3 = cpu_map_workspace_bytes(batch, l, n, 2), ws2 = cpu_map_workspace_bytes(batch, 2, n, 1);
+  int rc = c.ensure_ws(encrypt_workspace_bytes(n, l, batch));
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *rk = ar.take<uint32_t>((size_t)batch * 2 * 60);
+  uint32_t *f3 = ar.take<uint32_t>((size_t)batch * l * poly);
+  uint32_t *s2o = ar.take<uint32_t>((size_t)batch * 2 * poly);  // [b][2][3][n]: r, f0
+  uint32_t *rhat = ar.take<uint32_t>((size_t)batch * poly);
+  uint32_t *rhat_sh = ar.take<uint32_t>((size_t)batch * poly);
+  void *sws3 = ar.take<uint8_t>(ws3);
+  void *sws2 = ar.take<uint8_t>(ws2);
+  std::vector<uint32_t> k2 = expand_keys(batch, seeds2), k3 = expand_keys(batch, seeds3);
+  k2.insert(k2.end(), k3.begin(), k3.end());
+  CUFE_CUDA(cudaMemcpyAsync(rk, k2.data(), k2.size() * 4, cudaMemcpyHostToDevice, s));
+  rc = sample_cpu_map(1, batch, rk, 2, n, s2o, sws2, c.d_status, c.num_sms, s);
+  if (rc) return rc;
+  rc = sample_cpu_map(2, batch, rk + (size_t)batch * 60, l, n, f3, sws3, c.d_status, c.num_sms, s);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMemcpy2DAsync(rhat, poly * 4, s2o, 2 * poly * 4, poly * 4, batch, cudaMemcpyDeviceToDevice, s));
+  rc = ntt_fwd_shoup_launch(c.ring.args, rhat, rhat_sh, (long long)batch * 3, s);
+  if (rc) return rc;
+  return encrypt_tail(c, batch, d_x, d_mpk, rhat, rhat_sh, (long long)poly, f3, (long long)l * poly, s2o + poly,
+                      (long long)2 * poly, d_ct, s);
+}
+
+int ctx_encrypt_gpu_map(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seed2,
+                        uint32_t *d_ct, cudaStream_t s) {
+  if (batch < 1 || !seed2) return CUFE_ERR_INVALID;
+  const int n = c.n, l = c.l;
+  const size_t poly = (size_t)3 * n;
+  int rc = c.ensure_ws(((size_t)l * poly + 3 * poly) * 4 + 60 * 4 + 8 * 256);
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *rk = ar.take<uint32_t>(60);
+  uint32_t *f3 = ar.take<uint32_t>((size_t)l * poly);
+  uint32_t *r = ar.take<uint32_t>(poly);
+  uint32_t *rhat = ar.take<uint32_t>(poly);
+  uint32_t *rhat_sh = ar.take<uint32_t>(poly);
+  uint32_t keys[60];
+  aes_key_expand(seed2, keys);
+  CUFE_CUDA(cudaMemcpyAsync(rk, keys, sizeof(keys), cudaMemcpyHostToDevice, s));
+  // r and f_0 come from the same key and counters (src/rlwe_sife_gpu.cu:135-147), f_i from the
+  // same key with polynomial index i (src/sample_gpu.cu:217-289); every instance shares them.
+  rc = sample_gpu_map(1, rk, 0, 1, n, r, c.d_status, s);
+  if (rc) return rc;
+  rc = sample_gpu_map(2, rk, 0, l, n, f3, c.d_status, s);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMemcpyAsync(rhat, r, poly * 4, cudaMemcpyDeviceToDevice, s));
+  rc = ntt_fwd_shoup_launch(c.ring.args, rhat, rhat_sh, 3, s);
+  if (rc) return rc;
+  return encrypt_tail(c, batch, d_x, d_mpk, rhat, rhat_sh, 0, f3, 0, r, 0, d_ct, s);
+}
+
+int ctx_keygen(Ctx &c, int nkeys, const uint32_t *d_y, int y_signed, const uint32_t *d_msk, uint32_t *d_sky,
+               cudaStream_t s) {
+  if (nkeys < 1) return CUFE_ERR_INVALID;
+  constexpr int KCH = 4;
+  const SchemeArgs sa = scheme_args(c);
+  const size_t smem = (size_t)2 * KCH * c.l * 4;
+  if (smem > 200 * 1024) return CUFE_ERR_INVALID;
+  CUFE_CUDA(cudaFuncSetAttribute(k_keygen<KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((c.n + 255) / 256, 3, (nkeys + KCH - 1) / KCH);
+  k_keygen<KCH><<<grid, 256, smem, s>>>(d_y, y_signed, nkeys, d_msk, d_sky, c.n, sa);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s) {
+  if (nct < 1 || nkeys < 1) return CUFE_ERR_INVALID;
+  const int n = c.n, l = c.l;
+  const size_t poly = (size_t)3 * n;
+  int rc = c.ensure_ws(((size_t)nct * poly + 2 * (size_t)nkeys * poly) * 4 + 4 * 256);
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *clhat = ar.take<uint32_t>((size_t)nct * poly);
+  uint32_t *skhat = ar.take<uint32_t>((size_t)nkeys * poly);
+  uint32_t *skhat_sh = ar.take<uint32_t>((size_t)nkeys * poly);
+  CUFE_CUDA(cudaMemcpy2DAsync(clhat, poly * 4, d_ct + (size_t)l * poly, (size_t)(l + 1) * poly * 4, poly * 4, nct,
+                              cudaMemcpyDeviceToDevice, s));
+  rc = ntt_launch(c.ring.args, clhat, (long long)nct * 3, false, s);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMemcpyAsync(skhat, d_sky, (size_t)nkeys * poly * 4, cudaMemcpyDeviceToDevice, s));
+  rc = ntt_fwd_shoup_launch(c.ring.args, skhat, skhat_sh, (long long)nkeys * 3, s);
+  if (rc) return rc;
+  const long long nwork = (long long)nct * nkeys * 3;
+  const SchemeArgs sa = scheme_args(c);
+  return dispatch_logn(c.ring.logn, [&](auto L) {
+    constexpr int LOGN = decltype(L)::value;
+    constexpr int G = ppc<LOGN>();
+    const size_t smem = (size_t)G * (NttPlan<LOGN>::N + 2 * l) * 4;
+    if (smem > 200 * 1024) return (int)CUFE_ERR_INVALID;
+    CUFE_CUDA(cudaFuncSetAttribute(k_decrypt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_decrypt<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
+        d_ct, clhat, skhat, skhat_sh, d_y, y_signed, nct, nkeys, d_dy, nwork, sa);
+    CUFE_CUDA(cudaGetLastError());
+    return (int)CUFE_OK;
+  });
+}
+
+int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s) {
+  if (count < 1 || ncoeff < 1 || ncoeff > c.n) return CUFE_ERR_INVALID;
+  DecodeArgs d;
+  d.q0 = kRefPrimes[0];
+  d.q1 = kRefPrimes[1];
+  d.q2 = kRefPrimes[2];
+  d.c1 = c.crt_c1;
+  d.c1_sh = c.crt_c1_sh;
+  d.c2 = c.crt_c2;
+  d.c2_sh = c.crt_c2_sh;
+  d.mu2 = (uint64_t)(((u128)1 << 64) / kRefPrimes[2]);
+  d.q01 = (uint64_t)kRefPrimes[0] * kRefPrimes[1];
+  d.qlo = (unsigned long long)(uint64_t)c.q;
+  d.qhi = (unsigned long long)(uint64_t)(c.q >> 64);
+  d.hlo = (unsigned long long)(uint64_t)c.qhalf;
+  d.hhi = (unsigned long long)(uint64_t)(c.qhalf >> 64);
+  d.p = c.p;
+  d.n = c.n;
+  const long long total = (long long)count * ncoeff;
+  k_decode<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_dy, count, ncoeff, d_out, d);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
+                       cudaStream_t s) {
+  if (sig < 0 || sig > 2 || nstreams < 1 || calls < 1) return CUFE_ERR_INVALID;
+  const size_t sws = cpu_map_workspace_bytes(nstreams, calls, c.n, sig);
+  int rc = c.ensure_ws(sws + (size_t)nstreams * 60 * 4 + 512);
+  if (rc) return rc;
+  Arena ar(c.ws);
+  uint32_t *rk = ar.take<uint32_t>((size_t)nstreams * 60);
+  void *w = ar.take<uint8_t>(sws);
+  std::vector<uint32_t> k = expand_keys(nstreams, keys);
+  CUFE_CUDA(cudaMemcpyAsync(rk, k.data(), k.size() * 4, cudaMemcpyHostToDevice, s));
+  return sample_cpu_map(sig, nstreams, rk, calls, c.n, d_out, w, c.d_status, c.num_sms, s);
+}
+
+int ctx_sample_gpu_map(Ctx &c, int sig, const uint8_t *key, int poly0, int npolys, uint32_t *d_out,
+                       cudaStream_t s) {
+  if (sig < 0 || sig > 2 || npolys < 1 || poly0 < 0 || !key) return CUFE_ERR_INVALID;
+  int rc = c.ensure_ws(256 + 60 * 4);
+  if (rc) return rc;
+  uint32_t k[60];
+  aes_key_expand(key, k);
+  CUFE_CUDA(cudaMemcpyAsync(c.ws, k, sizeof(k), cudaMemcpyHostToDevice, s));
+  return sample_gpu_map(sig, reinterpret_cast<uint32_t *>(c.ws), poly0, npolys, c.n, d_out, c.d_status, s);
+}
+
+int ctx_sample_polya(Ctx &c, const uint8_t *seed, uint32_t *d_a, cudaStream_t s) {
+  if (!seed) return CUFE_ERR_INVALID;
+  int rc = c.ensure_ws(256 + 60 * 4);
+  if (rc) return rc;
+  uint32_t k[60];
+  aes_key_expand(seed, k);
+  CUFE_CUDA(cudaMemcpyAsync(c.ws, k, sizeof(k), cudaMemcpyHostToDevice, s));
+  return sample_polya(reinterpret_cast<uint32_t *>(c.ws), c.n, d_a, s);
+}
+
+}  // namespace cufe

@@ -1,0 +1,147 @@
+// ntt.cuh -- negacyclic NTT / INTT cores for one residue polynomial per thread group.
+//
+// Transform (reference: src/ntt.c:38-114): forward Cooley-Tukey with the psi powers
+// merged (natural order in, bit-reversed order out), inverse Gentleman-Sande (bit-reversed
+// in, natural out) including the factor n^-1.  Any exact implementation of this linear map
+// gives the reference's values after canonical reduction, so the loop order is free.
+//
+// B200 design: n/16 threads per residue polynomial, 16 coefficients per thread held in
+// registers.  The log2(n) butterfly stages are grouped into passes of up to 4 stages
+// (radix 16); a pass touches only the 16 coefficients of a thread, and consecutive passes
+// exchange coefficients through shared memory (one __syncthreads per exchange) with an
+// XOR swizzle (j ^ ((j >> 4) & 31)) that keeps every exchange pattern of these plans free
+// of bank conflicts without padding.  The smaller pass (log2(n) mod 4 stages) comes first so that the strided
+// passes are the early ones, whose warps touch 32 consecutive words.  Twiddles use
+// Shoup's precomputed quotient (1 mul.hi + 2 mul.lo per product) and residues stay
+// canonical in [0, q), q < 2^31.  The inverse folds n^-1 into its last stage.
+#pragma once
+#include "cufe_internal.cuh"
+
+namespace cufe {
+
+template <int LOGN>
+struct NttPlan {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int T = N / 16;  // threads per residue polynomial
+  static constexpr int NP = (LOGN + 3) / 4;
+  static constexpr int R0 = LOGN - 4 * (NP - 1);
+  static constexpr int SMEM_WORDS = N;
+  __host__ __device__ static constexpr int radix_bits(int p) { return p == 0 ? R0 : 4; }
+  __host__ __device__ static constexpr int first_stage(int p) { return p == 0 ? 0 : R0 + 4 * (p - 1); }
+  // coefficient index held in register e by thread th during pass PASS
+  template <int PASS>
+  __device__ __forceinline__ static int idx(int th, int e) {
+    constexpr int rb = radix_bits(PASS), s0 = first_stage(PASS);
+    constexpr int plo = LOGN - s0 - rb, phi = LOGN - 1 - s0;
+    const int v = e >> rb, M = e & ((1 << rb) - 1);
+    const int U = v * T + th;
+    const int H = U >> plo, L = U & ((1 << plo) - 1);
+    return (H << (phi + 1)) | (M << plo) | L;
+  }
+  __device__ __forceinline__ static int swz(int j) { return j ^ ((j >> 4) & 31); }
+};
+
+template <int LOGN, int FROM, int TO>
+__device__ __forceinline__ void ntt_exchange(uint32_t (&a)[16], uint32_t *sm, int th) {
+  using P = NttPlan<LOGN>;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) sm[P::swz(P::template idx<FROM>(th, e))] = a[e];
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = sm[P::swz(P::template idx<TO>(th, e))];
+}
+
+struct InvScale {
+  uint32_t ninv, ninv_sh, w1n, w1n_sh;
+};
+
+// stage LS of pass PASS (CT stage s = first_stage(PASS) + LS; the inverse runs the same
+// butterfly positions with Gentleman-Sande butterflies and psi^-1 twiddles)
+template <int LOGN, int PASS, int LS, bool INV>
+__device__ __forceinline__ void ntt_stage(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *__restrict__ tw,
+                                          const uint32_t *__restrict__ twsh, const InvScale &sc) {
+  using P = NttPlan<LOGN>;
+  constexpr int rb = P::radix_bits(PASS), s0 = P::first_stage(PASS), plo = LOGN - s0 - rb;
+  constexpr int s = s0 + LS, half = 1 << (rb - 1 - LS), nv = 16 >> rb, ng = 1 << LS;
+#pragma unroll
+  for (int v = 0; v < nv; ++v) {
+    const int H = (v * P::T + th) >> plo;
+#pragma unroll
+    for (int g = 0; g < ng; ++g) {
+      if constexpr (INV && s == 0) {
+#pragma unroll
+        for (int b = 0; b < half; ++b) {
+          const int e1 = (v << rb) + g * 2 * half + b, e2 = e1 + half;
+          const uint32_t U = a[e1], V = a[e2];
+          a[e1] = shoup_mul(U + V, sc.ninv, sc.ninv_sh, q);
+          a[e2] = shoup_mul(U - V + q, sc.w1n, sc.w1n_sh, q);
+        }
+      } else {
+        const int ti = (1 << s) + ((H << LS) | g);
+        const uint32_t w = __ldg(tw + ti), wsh = __ldg(twsh + ti);
+#pragma unroll
+        for (int b = 0; b < half; ++b) {
+          const int e1 = (v << rb) + g * 2 * half + b, e2 = e1 + half;
+          if constexpr (!INV) {
+            const uint32_t V = shoup_mul(a[e2], w, wsh, q);
+            const uint32_t U = a[e1];
+            a[e1] = mod_add(U, V, q);
+            a[e2] = mod_sub(U, V, q);
+          } else {
+            const uint32_t U = a[e1], V = a[e2];
+            a[e1] = mod_add(U, V, q);
+            a[e2] = shoup_mul(U - V + q, w, wsh, q);
+          }
+        }
+      }
+    }
+  }
+}
+
+template <int LOGN, int PASS, int LS>
+__device__ __forceinline__ void ntt_fwd_stages(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *tw,
+                                               const uint32_t *twsh) {
+  ntt_stage<LOGN, PASS, LS, false>(a, th, q, tw, twsh, InvScale{});
+  if constexpr (LS + 1 < NttPlan<LOGN>::radix_bits(PASS)) ntt_fwd_stages<LOGN, PASS, LS + 1>(a, th, q, tw, twsh);
+}
+template <int LOGN, int PASS>
+__device__ __forceinline__ void ntt_fwd_passes(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q, const uint32_t *tw,
+                                               const uint32_t *twsh) {
+  if constexpr (PASS > 0) ntt_exchange<LOGN, PASS - 1, PASS>(a, sm, th);
+  ntt_fwd_stages<LOGN, PASS, 0>(a, th, q, tw, twsh);
+  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_fwd_passes<LOGN, PASS + 1>(a, sm, th, q, tw, twsh);
+}
+template <int LOGN, int PASS, int LS>
+__device__ __forceinline__ void ntt_inv_stages(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *tw,
+                                               const uint32_t *twsh, const InvScale &sc) {
+  ntt_stage<LOGN, PASS, LS, true>(a, th, q, tw, twsh, sc);
+  if constexpr (LS > 0) ntt_inv_stages<LOGN, PASS, LS - 1>(a, th, q, tw, twsh, sc);
+}
+template <int LOGN, int PASS>
+__device__ __forceinline__ void ntt_inv_passes(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q, const uint32_t *tw,
+                                               const uint32_t *twsh, const InvScale &sc) {
+  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_exchange<LOGN, PASS + 1, PASS>(a, sm, th);
+  ntt_inv_stages<LOGN, PASS, NttPlan<LOGN>::radix_bits(PASS) - 1>(a, th, q, tw, twsh, sc);
+  if constexpr (PASS > 0) ntt_inv_passes<LOGN, PASS - 1>(a, sm, th, q, tw, twsh, sc);
+}
+
+// Registers a[] hold the pass-0 layout on entry and the last-pass layout (16 consecutive
+// coefficients th*16 .. th*16+15) on exit.  sm: this polynomial's SMEM_WORDS scratch.
+template <int LOGN>
+__device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,
+                                             const uint32_t *__restrict__ psi,
+                                             const uint32_t *__restrict__ psh) {
+  ntt_fwd_passes<LOGN, 0>(a, sm, th, q, psi, psh);
+}
+
+// Registers hold the last-pass layout (16 consecutive coefficients) on entry and the
+// pass-0 layout on exit.  Inputs must be canonical residues.
+template <int LOGN>
+__device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,
+                                             const uint32_t *__restrict__ ipsi,
+                                             const uint32_t *__restrict__ ipsh, uint32_t ninv,
+                                             uint32_t ninv_sh, uint32_t w1n, uint32_t w1n_sh) {
+  ntt_inv_passes<LOGN, NttPlan<LOGN>::NP - 1>(a, sm, th, q, ipsi, ipsh, InvScale{ninv, ninv_sh, w1n, w1n_sh});
+}
+
+}  // namespace cufe

@@ -1,0 +1,700 @@
+// sampler.cu -- AES-256-CTR keystreams and the discrete Gaussian / uniform samplers.
+//
+// Two counter-to-sample mappings are implemented, both bit-exact:
+//
+//  * CPU mapping (src/gauss.c + src/aes256ctr.c): one AES-CTR stream per context; every
+//    gaussian_sampler_* call consumes 384-byte refills (24 counter blocks) in order, takes
+//    the accepted candidates in order and drops the rest of its last refill.  The stream is
+//    sequential by construction, so it is computed in three parallel phases: (1) every
+//    refill's 8 candidates and accept mask for a generous refill range (the AES work, one
+//    thread per refill), (2) a per-stream exclusive scan of accept counts and a one-warp
+//    walk that finds where each call starts (each call starts at a fresh refill), (3) a
+//    scatter of the accepted candidates to their coefficient positions as residues.
+//  * GPU mapping (src/sample_gpu.cu, src/AES.cuh): thread t of polynomial p owns coefficients
+//    8t..8t+7 and draws chained-AES refills from counter p*5*T*24 + rep*T*24 + t*24.
+#include "aes.cuh"
+#include "sampler.cuh"
+#include "sampler_host.h"
+
+#include <algorithm>
+
+namespace cufe {
+
+namespace {
+
+__device__ __forceinline__ uint64_t le64_of(uint32_t be_lo, uint32_t be_hi) {
+  return (uint64_t)bswap32(be_lo) | ((uint64_t)bswap32(be_hi) << 32);
+}
+
+// ------------------------------------------------------------------ CPU mapping, phase 1
+
+template <int SIG>
+__device__ __noinline__ void uniform_slow(const uint32_t *U, uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
+                                          const AesCtx &c, uint32_t *status) {
+  uint32_t rk[60];
+#pragma unroll
+  for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
+  int w = 0;
+  for (int j = 0; j < 8; ++j) {
+    uint32_t x = 0;
+    for (;;) {
+      if (w >= 46) {  // would read beyond the 384-byte refill: undefined in the reference
+        atomicOr(status, kStatusUniformOverrun);
+        x = 0;
+        break;
+      }
+      if (w < 22) {
+        x = U[w];
+      } else {
+        const int byte = 200 + 4 * w;
+        uint32_t W[4];
+        aes256_ctr_block(W, 0u, cb + (uint32_t)(byte >> 4), rk, c);
+        x = bswap32(W[(byte >> 2) & 3]);
+      }
+      ++w;
+      if (uniform_ok<SIG>(x)) break;
+    }
+    y[j] = uniform_reduce<SIG>(x);
+  }
+}
+
+// One refill of the CPU mapping: blocks needed for S1/S2 are 2-6 and 8-17 (bytes 32..287);
+// the 126-bit CDT of the CPU S3 additionally reads bytes 0..31 / 100..131, fetched only
+// when a high word ties a table entry.
+template <int SIG, bool FULL, int VAR>
+__global__ void __launch_bounds__(512, 1)
+    k_cand_cpu(const uint32_t *__restrict__ rkeys, uint32_t nstreams, uint32_t refills, double kinv,
+               int64_t *__restrict__ cand, uint8_t *__restrict__ amask, uint32_t *__restrict__ status) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  aes_fill_tables(smem);
+  __syncthreads();
+  const AesCtx c{smem, (threadIdx.x & 31u) * 4u};
+  const uint32_t total = nstreams * refills;
+  uint32_t rk[60];
+  uint32_t cur = 0xffffffffu;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const uint32_t st = g / refills, t = g - st * refills;
+    if (st != cur) {
+#pragma unroll
+      for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkeys + (size_t)st * 60 + i);
+      cur = st;
+    }
+    const uint32_t cb = t * 24u;
+    uint32_t W[4];
+    // ---- uniform words (bytes 200..287) and the sign byte 280
+    uint32_t U[22], keep0, keep1;
+    aes256_ctr_block(W, 0u, cb + 12u, rk, c);
+    keep0 = W[0];
+    keep1 = W[1];
+    U[0] = bswap32(W[2]);
+    U[1] = bswap32(W[3]);
+#pragma unroll
+    for (int b = 13; b < 18; ++b) {
+      aes256_ctr_block(W, 0u, cb + (uint32_t)b, rk, c);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) U[2 + 4 * (b - 13) + i] = bswap32(W[i]);
+    }
+    const uint32_t k8 = U[20] & 0xffu;
+    uint32_t y[8];
+    bool fast = true;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) fast &= uniform_ok<SIG>(U[i]);
+    if (fast) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) y[i] = uniform_reduce<SIG>(U[i]);
+    } else {
+      uint32_t Ul[22], yl[8];
+#pragma unroll
+      for (int i = 0; i < 22; ++i) Ul[i] = U[i];
+      uniform_slow<SIG>(Ul, yl, cb, rkeys + (size_t)st * 60, c, status);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) y[i] = yl[i];
+    }
+    uint64_t z[8];
+    uint32_t acc = 0;
+    // ---- lanes 0..3: CDT high words at 32..63, Bernoulli bytes 64..99
+    {
+      uint32_t A[4], B[4];
+      aes256_ctr_block(A, 0u, cb + 2u, rk, c);
+      aes256_ctr_block(B, 0u, cb + 3u, rk, c);
+      const uint64_t r2[4] = {le64_of(A[0], A[1]), le64_of(A[2], A[3]), le64_of(B[0], B[1]),
+                              le64_of(B[2], B[3])};
+      uint32_t x[4];
+      bool low = false;
+      if (FULL) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) low |= cdt_needs_low(r2[i]);
+      }
+      if (FULL && low) {
+        aes256_ctr_block(A, 0u, cb + 0u, rk, c);
+        aes256_ctr_block(B, 0u, cb + 1u, rk, c);
+        const uint64_t r1[4] = {le64_of(A[0], A[1]), le64_of(A[2], A[3]), le64_of(B[0], B[1]),
+                                le64_of(B[2], B[3])};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<FULL>(r2[i], r1[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<false>(r2[i], 0);
+      }
+      uint32_t M4[4], M5[4], M6[4];
+      aes256_ctr_block(M4, 0u, cb + 4u, rk, c);
+      aes256_ctr_block(M5, 0u, cb + 5u, rk, c);
+      aes256_ctr_block(M6, 0u, cb + 6u, rk, c);
+      const uint64_t rm[4] = {le64_of(M4[0], M4[1]), le64_of(M4[2], M4[3]), le64_of(M5[0], M5[1]),
+                              le64_of(M5[2], M5[3])};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t rexp = (M6[0] >> (24 - 8 * i)) & 0xffu;
+        const bool b = candidate<SIG, VAR>(x[i], y[i], rm[i], rexp, kinv, z[i]);
+        const uint32_t k = (k8 >> i) & 1u;
+        acc |= (uint32_t)accept_final(b, z[i], k) << i;
+      }
+      // ---- lanes 4..7: CDT high words at 132..163, Bernoulli bytes 164..199
+      uint32_t B8[4], B9[4], B10[4], B11[4];
+      aes256_ctr_block(B8, 0u, cb + 8u, rk, c);
+      aes256_ctr_block(B9, 0u, cb + 9u, rk, c);
+      aes256_ctr_block(B10, 0u, cb + 10u, rk, c);
+      const uint64_t s2[4] = {le64_of(B8[1], B8[2]), le64_of(B8[3], B9[0]), le64_of(B9[1], B9[2]),
+                              le64_of(B9[3], B10[0])};
+      bool low2 = false;
+      if (FULL) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) low2 |= cdt_needs_low(s2[i]);
+      }
+      if (FULL && low2) {
+        uint32_t B7[4];
+        aes256_ctr_block(B7, 0u, cb + 7u, rk, c);
+        const uint64_t s1[4] = {le64_of(M6[1], M6[2]), le64_of(M6[3], B7[0]), le64_of(B7[1], B7[2]),
+                                le64_of(B7[3], B8[0])};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<FULL>(s2[i], s1[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<false>(s2[i], 0);
+      }
+      aes256_ctr_block(B11, 0u, cb + 11u, rk, c);
+      const uint64_t sm[4] = {le64_of(B10[1], B10[2]), le64_of(B10[3], B11[0]), le64_of(B11[1], B11[2]),
+                              le64_of(B11[3], keep0)};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t rexp = (keep1 >> (24 - 8 * i)) & 0xffu;
+        const bool b = candidate<SIG, VAR>(x[i], y[4 + i], sm[i], rexp, kinv, z[4 + i]);
+        const uint32_t k = (k8 >> (4 + i)) & 1u;
+        acc |= (uint32_t)accept_final(b, z[4 + i], k) << (4 + i);
+      }
+    }
+    int64_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t zi = (int64_t)z[i];
+      v[i] = ((k8 >> i) & 1u) ? -zi : zi;
+    }
+    longlong2 *dst = reinterpret_cast<longlong2 *>(cand + (size_t)g * 8);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = make_longlong2(v[2 * i], v[2 * i + 1]);
+    amask[g] = (uint8_t)acc;
+  }
+}
+
+// ------------------------------------------------------------------ CPU mapping, phase 2
+
+constexpr int kScanTile = 4096;  // refills per scan tile (512 threads x 8)
+
+// per-tile exclusive scan of accept counts; E_local[t], tile sums
+__global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ amask, uint32_t refills,
+                                                    uint32_t tiles, uint32_t *__restrict__ elocal,
+                                                    uint32_t *__restrict__ tile_sum) {
+  __shared__ uint32_t wsum[16];
+  const uint32_t st = blockIdx.y, tile = blockIdx.x;
+  const uint32_t base = tile * kScanTile + threadIdx.x * 8;
+  uint32_t cnt[8], tot = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint32_t t = base + i;
+    cnt[i] = t < refills ? __popc(amask[(size_t)st * refills + t]) : 0u;
+    tot += cnt[i];
+  }
+  // block exclusive scan of per-thread totals
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < 16 ? wsum[lane] : 0u, si = s;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, si, o);
+      if (lane >= o) si += v;
+    }
+    if (lane < 16) wsum[lane] = si - s;
+    if (lane == 15) tile_sum[(size_t)st * tiles + tile] = si;
+  }
+  __syncthreads();
+  uint32_t run = wsum[wid] + inc - tot;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint32_t t = base + i;
+    if (t < refills) elocal[(size_t)st * refills + t] = run;
+    run += cnt[i];
+  }
+}
+
+// exclusive scan of tile sums per stream (one block per stream)
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *__restrict__ tile_sum, uint32_t tiles) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t carry;
+  const uint32_t st = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < tiles; b0 += 1024) {
+    const uint32_t i = b0 + threadIdx.x;
+    const uint32_t v = i < tiles ? tile_sum[(size_t)st * tiles + i] : 0u;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
+    }
+    if (lane == 31) wsum[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t s = wsum[lane], si = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, si, o);
+        if (lane >= o) si += u;
+      }
+      wsum[lane] = si - s;
+    }
+    __syncthreads();
+    const uint32_t excl = carry + wsum[wid] + inc - v;
+    if (i < tiles) tile_sum[(size_t)st * tiles + i] = excl;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = excl + v;
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint32_t prefix_at(const uint32_t *elocal, const uint32_t *tile_off,
+                                              const uint8_t *amask, uint32_t refills, uint32_t tiles,
+                                              uint32_t st, uint32_t t) {
+  // exclusive prefix E(t) for t in [0, refills]
+  if (t < refills) return elocal[(size_t)st * refills + t] + tile_off[(size_t)st * tiles + t / kScanTile];
+  const uint32_t l = refills - 1;
+  return elocal[(size_t)st * refills + l] + tile_off[(size_t)st * tiles + l / kScanTile] +
+         __popc(amask[(size_t)st * refills + l]);
+}
+
+// one warp per stream: call c starts at a fresh refill a_c; it ends at the first refill e
+// whose inclusive prefix reaches E(a_c) + n; a_{c+1} = e + 1.
+__global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__restrict__ tile_off,
+                       const uint8_t *__restrict__ amask, uint32_t refills, uint32_t tiles, uint32_t calls,
+                       uint32_t n, uint32_t guess, uint32_t nstreams, uint32_t *__restrict__ call_start,
+                       uint32_t *__restrict__ status) {
+  const uint32_t st = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (st >= nstreams) return;  // whole warps only
+  uint32_t a = 0;
+  bool bad = false;
+  uint32_t c = 0;
+  for (; c < calls && !bad; ++c) {
+    const uint32_t base = prefix_at(elocal, tile_off, amask, refills, tiles, st, a);
+    const uint32_t target = base + n;
+    // smallest e >= a whose inclusive prefix reaches target (monotone in e), searched in
+    // windows of 32 refills around the expected call length; `known` is a position already
+    // seen to satisfy.  Upward moves stop at the refill range, downward moves at a.
+    uint32_t lo = a + (guess > 16 ? guess - 16 : 0);
+    int64_t known = -1;
+    uint32_t e = 0;
+    for (int it = 0;; ++it) {
+      if (it > (1 << 22)) {  // cannot happen for a monotone prefix; bounded regardless
+        bad = true;
+        break;
+      }
+      const uint32_t j = lo + lane;
+      const bool ok = (j < refills) && prefix_at(elocal, tile_off, amask, refills, tiles, st, j + 1) >= target;
+      const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+      if (bal == 0) {
+        if (known >= 0) {
+          e = (uint32_t)known;
+          break;
+        }
+        if (lo + 32 >= refills) {
+          bad = true;
+          break;
+        }
+        lo += 32;
+        continue;
+      }
+      const int first = __ffs(bal) - 1;
+      if (first > 0 || lo == a) {
+        e = lo + first;
+        break;
+      }
+      known = lo;
+      lo = lo > a + 32 ? lo - 32 : a;
+    }
+    if (bad) break;
+    if (lane == 0) call_start[(size_t)st * (calls + 1) + c] = a;
+    a = e + 1;
+  }
+  if (lane == 0) {
+    if (bad) atomicOr(status, kStatusRefillsExhausted);
+    for (uint32_t r = bad ? c : calls; r <= calls; ++r)
+      call_start[(size_t)st * (calls + 1) + r] = bad ? refills : a;
+  }
+}
+
+// ------------------------------------------------------------------ CPU mapping, phase 3
+
+struct ModArgs {
+  uint32_t q[3];
+  uint64_t mu[3];
+};
+
+__device__ __forceinline__ uint32_t signed_residue(int64_t s, uint32_t q, uint64_t mu) {
+  if (s >= 0) return mod_u64((uint64_t)s, mu, q);
+  const uint32_t r = mod_u64((uint64_t)(-s), mu, q);
+  return r ? q - r : 0u;
+}
+
+// one CTA per (call, stream): accepted candidates of refills [a_c, a_{c+1}) in order
+__global__ void __launch_bounds__(256) k_scatter(const int64_t *__restrict__ cand, const uint8_t *__restrict__ amask,
+                                                 const uint32_t *__restrict__ elocal,
+                                                 const uint32_t *__restrict__ tile_off,
+                                                 const uint32_t *__restrict__ call_start, uint32_t refills,
+                                                 uint32_t tiles, uint32_t calls, uint32_t n, ModArgs m,
+                                                 uint32_t *__restrict__ out) {
+  const uint32_t c = blockIdx.x, st = blockIdx.y;
+  const uint32_t a = call_start[(size_t)st * (calls + 1) + c];
+  const uint32_t b = call_start[(size_t)st * (calls + 1) + c + 1];
+  if (a >= refills) return;
+  const uint32_t base = prefix_at(elocal, tile_off, amask, refills, tiles, st, a);
+  uint32_t *o = out + ((size_t)st * calls + c) * 3 * n;
+  for (uint32_t t = a + threadIdx.x; t < b && t < refills; t += blockDim.x) {
+    const uint32_t g = st * refills + t;
+    uint32_t msk = amask[g];
+    uint32_t pos = prefix_at(elocal, tile_off, amask, refills, tiles, st, t) - base;
+    const int64_t *cv = cand + (size_t)g * 8;
+    while (msk) {
+      const int i = __ffs(msk) - 1;
+      msk &= msk - 1;
+      if (pos < n) {
+        const int64_t s = cv[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[j * n + pos] = signed_residue(s, m.q[j], m.mu[j]);
+      }
+      ++pos;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ GPU mapping
+
+// chained AES refill of the GPU mapping (src/AES.cuh:380-435): 18 blocks (bytes 0..287)
+// into buf; blocks 18..23 only when a uniform draw needs them.
+__device__ __forceinline__ void chain_blocks(uint32_t *buf, int from, int to, uint32_t &s0, uint32_t &s1,
+                                             uint32_t &s2, uint32_t &s3, const uint32_t (&rk)[60],
+                                             const AesCtx &c) {
+  for (int m = from; m < to; ++m) {
+    aes256_rounds(s0, s1, s2, s3, rk, c);
+    buf[4 * m] = s0;
+    buf[4 * m + 1] = s1;
+    buf[4 * m + 2] = s2;
+    buf[4 * m + 3] = s3;
+  }
+}
+
+template <int SIG>
+__global__ void __launch_bounds__(256)
+    k_gauss_gpu_map(const uint32_t *__restrict__ rkey, uint32_t poly0, uint32_t npolys, uint32_t n, double kinv,
+                    ModArgs m, uint32_t *__restrict__ out, uint32_t *__restrict__ status) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  aes_fill_tables(smem);
+  __syncthreads();
+  const AesCtx c{smem, (threadIdx.x & 31u) * 4u};
+  uint32_t rk[60];
+#pragma unroll
+  for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkey + i);
+  const uint32_t T = n / 8;
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= npolys * T) return;
+  const uint32_t p = gid / T, t = gid - p * T, poly = poly0 + p;
+  uint32_t buf[96];
+  uint32_t y[8], x[8], acc = 0, k8 = 0;
+  uint64_t z[8];
+  uint32_t i = 8, rep = 0;
+  uint32_t *o = out + (size_t)p * 3 * n;
+  bool gave_up = false;
+  for (uint32_t j = 0; j < 8 && !gave_up; ++j) {
+    uint32_t k = 0;
+    for (;;) {
+      if (i == 8) {
+        if (rep >= kMaxRefillsPerThread) {  // never reached by a working sampler; bounded anyway
+          atomicOr(status, kStatusRefillCap);
+          gave_up = true;
+          break;
+        }
+        const uint32_t ctr = poly * 5u * T * 24u + rep * T * 24u + t * 24u;
+        uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2], s3 = ctr ^ rk[3];
+        aes256_rounds(s0, s1, s2, s3, rk, c);
+        buf[0] = s0; buf[1] = s1; buf[2] = s2; buf[3] = s3;
+        chain_blocks(buf, 1, 18, s0, s1, s2, s3, rk, c);
+        int have = 18;
+        // uniform words from byte 200 (word 50)
+        int w = 0;
+        for (int jj = 0; jj < 8; ++jj) {
+          uint32_t xx;
+          for (;;) {
+            const int wi = 50 + w;
+            if (wi >= 96) {
+              atomicOr(status, kStatusUniformOverrun);
+              xx = 0;
+              break;
+            }
+            if ((wi >> 2) >= have) {
+              chain_blocks(buf, have, have + 1, s0, s1, s2, s3, rk, c);
+              ++have;
+            }
+            xx = bswap32(buf[wi]);
+            ++w;
+            if (uniform_ok<SIG>(xx)) break;
+          }
+          y[jj] = uniform_reduce<SIG>(xx);
+        }
+        for (int h = 0; h < 2; ++h) {
+          const int bw = 25 * h;  // word offset of r + 100*h
+          for (int ln = 0; ln < 4; ++ln) {
+            const uint64_t r2 = ((uint64_t)bswap32(buf[bw + 8 + 2 * ln])) |
+                                ((uint64_t)bswap32(buf[bw + 9 + 2 * ln]) << 32);
+            x[4 * h + ln] = cdt_sample<false>(r2, 0);
+          }
+        }
+        k8 = buf[70] >> 24;  // byte 280
+        acc = 0;
+        for (int h = 0; h < 2; ++h) {
+          const int bw = 25 * h;
+          const uint32_t ew = buf[bw + 24];  // bytes 96..99 (+100 h)
+          for (int ln = 0; ln < 4; ++ln) {
+            const uint64_t rm = ((uint64_t)bswap32(buf[bw + 16 + 2 * ln])) |
+                                ((uint64_t)bswap32(buf[bw + 17 + 2 * ln]) << 32);
+            const uint32_t rexp = (ew >> (24 - 8 * ln)) & 0xffu;
+            uint64_t zz;
+            const bool b = candidate<SIG, 2>(x[4 * h + ln], y[4 * h + ln], rm, rexp, kinv, zz);
+            z[4 * h + ln] = zz;
+            acc |= (uint32_t)b << (4 * h + ln);
+          }
+        }
+        i = 0;
+        ++rep;
+      }
+      k = (k8 >> i) & 1u;
+      ++i;
+      if (accept_final((acc >> (i - 1)) & 1u, z[i - 1], k)) break;
+    }
+    if (gave_up) break;
+    const int64_t zs = (int64_t)z[i - 1];
+    const int64_t s = k ? -zs : zs;
+    const uint32_t pos = 8 * t + j;
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) o[jj * n + pos] = signed_residue(s, m.q[jj], m.mu[jj]);
+  }
+}
+
+// ------------------------------------------------------------------ uniform a
+
+// sample_polya (src/sample.c:56-128): AES-CTR (nonce 0) bytes, a_i = le64(bytes 8i..8i+7) mod q_j
+__global__ void __launch_bounds__(256) k_polya(const uint32_t *__restrict__ rkey, uint32_t n, ModArgs m,
+                                               uint32_t *__restrict__ a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  aes_fill_tables(smem);
+  __syncthreads();
+  const AesCtx c{smem, (threadIdx.x & 31u) * 4u};
+  uint32_t rk[60];
+#pragma unroll
+  for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkey + i);
+  const uint32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= n / 2) return;
+  uint32_t W[4];
+  aes256_ctr_block(W, 0u, blk, rk, c);
+  const uint64_t v0 = le64_of(W[0], W[1]), v1 = le64_of(W[2], W[3]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    a[j * n + 2 * blk] = mod_u64(v0, m.mu[j], m.q[j]);
+    a[j * n + 2 * blk + 1] = mod_u64(v1, m.mu[j], m.q[j]);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+static ModArgs mod_args() {
+  ModArgs m;
+  for (int j = 0; j < 3; ++j) {
+    m.q[j] = kRefPrimes[j];
+    unsigned __int128 one = (unsigned __int128)1 << 64;
+    m.mu[j] = (uint64_t)(one / kRefPrimes[j]);
+  }
+  return m;
+}
+
+static double kinv_of(int sig) {
+  const uint64_t K = sigma_k(sig);
+  return -1.0 / (double)(int64_t)(K * K);
+}
+
+static uint8_t gmul8(uint8_t a, uint8_t b) {
+  uint8_t r = 0;
+  while (b) {
+    if (b & 1) r ^= a;
+    a = (uint8_t)((a << 1) ^ ((a & 0x80) ? 0x1b : 0));
+    b >>= 1;
+  }
+  return r;
+}
+
+void aes_key_expand(const uint8_t key[32], uint32_t w[60]) {
+  static uint8_t sbox[256];
+  static bool ready = false;
+  if (!ready) aes_sbox(sbox), ready = true;
+  uint8_t rc = 1;
+  for (int i = 0; i < 8; ++i)
+    w[i] = ((uint32_t)key[4 * i] << 24) | ((uint32_t)key[4 * i + 1] << 16) | ((uint32_t)key[4 * i + 2] << 8) |
+           key[4 * i + 3];
+  for (int i = 8; i < 60; ++i) {
+    uint32_t t = w[i - 1];
+    auto sub = [&](uint32_t v) {
+      return ((uint32_t)sbox[v >> 24] << 24) | ((uint32_t)sbox[(v >> 16) & 255] << 16) |
+             ((uint32_t)sbox[(v >> 8) & 255] << 8) | sbox[v & 255];
+    };
+    if (i % 8 == 0) {
+      t = sub((t << 8) | (t >> 24)) ^ ((uint32_t)rc << 24);
+      rc = gmul8(rc, 2);
+    } else if (i % 8 == 4) {
+      t = sub(t);
+    }
+    w[i] = w[i - 8] ^ t;
+  }
+}
+
+void aes_sbox(uint8_t out[256]) {
+  // FIPS-197 5.1.1: multiplicative inverse in GF(2^8) followed by the affine map
+  for (int x = 0; x < 256; ++x) {
+    uint8_t inv = 0;
+    if (x)
+      for (int y = 1; y < 256; ++y)
+        if (gmul8((uint8_t)x, (uint8_t)y) == 1) {
+          inv = (uint8_t)y;
+          break;
+        }
+    uint8_t s = inv;
+    for (int r = 1; r <= 4; ++r) s ^= (uint8_t)((inv << r) | (inv >> (8 - r)));
+    out[x] = s ^ 0x63;
+  }
+}
+
+int sampler_init_device() {
+  uint8_t sbox[256];
+  aes_sbox(sbox);
+  CUFE_CUDA(cudaMemcpyToSymbol(c_sbox, sbox, 256));
+  CUFE_CUDA(cudaFuncSetAttribute(k_cand_cpu<0, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_cand_cpu<1, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_cand_cpu<2, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_gauss_gpu_map<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_gauss_gpu_map<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_gauss_gpu_map<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  CUFE_CUDA(cudaFuncSetAttribute(k_polya, cudaFuncAttributeMaxDynamicSharedMemorySize, kAesSmemBytes));
+  return CUFE_OK;
+}
+
+// accepted candidates per 8-candidate refill of the CPU mapping, rounded down from oracle
+// measurements (5.44, 4.39, 3.09 for S1, S2, S3; the truncations of Q5 reject more at large K)
+static double mean_accept(int sig) { return sig == 0 ? 5.35 : (sig == 1 ? 4.3 : 3.0); }
+
+size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, int sig) {
+  const uint32_t R = cpu_map_refills(calls, n, sig);
+  const uint32_t tiles = (R + kScanTile - 1) / kScanTile;
+  size_t b = 0;
+  auto add = [&](size_t x) { b += (x + 255) & ~(size_t)255; };
+  add((size_t)nstreams * R * 64);        // candidates
+  add((size_t)nstreams * R);             // masks
+  add((size_t)nstreams * R * 4);         // local prefix
+  add((size_t)nstreams * tiles * 4);     // tile sums
+  add((size_t)nstreams * (calls + 1) * 4);  // call starts
+  return b;
+}
+
+uint32_t cpu_map_refills(uint32_t calls, uint32_t n, int sig) {
+  const double mu = mean_accept(sig);
+  const double need = (double)calls * ((double)n / mu + 1.0);
+  uint32_t R = (uint32_t)(need * 1.03) + 256;
+  return (R + 31) & ~31u;
+}
+
+int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
+                   uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s) {
+  const uint32_t R = cpu_map_refills(calls, n, sig);
+  const uint32_t tiles = (R + kScanTile - 1) / kScanTile;
+  if ((uint64_t)nstreams * R >= (1ull << 32) - 1) return CUFE_ERR_INVALID;
+  uint8_t *p = static_cast<uint8_t *>(ws);
+  auto take = [&](size_t x) {
+    uint8_t *r = p;
+    p += (x + 255) & ~(size_t)255;
+    return r;
+  };
+  int64_t *cand = reinterpret_cast<int64_t *>(take((size_t)nstreams * R * 64));
+  uint8_t *amask = take((size_t)nstreams * R);
+  uint32_t *elocal = reinterpret_cast<uint32_t *>(take((size_t)nstreams * R * 4));
+  uint32_t *tsum = reinterpret_cast<uint32_t *>(take((size_t)nstreams * tiles * 4));
+  uint32_t *cstart = reinterpret_cast<uint32_t *>(take((size_t)nstreams * (calls + 1) * 4));
+  const double kinv = kinv_of(sig);
+  const uint32_t total = nstreams * R;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (total + 511) / 512);
+  if (sig == 0)
+    k_cand_cpu<0, false, 0><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+  else if (sig == 1)
+    k_cand_cpu<1, false, 0><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+  else
+    k_cand_cpu<2, true, 1><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+  CUFE_CUDA(cudaGetLastError());
+  k_scan_tiles<<<dim3(tiles, nstreams), 512, 0, s>>>(amask, R, tiles, elocal, tsum);
+  k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles);
+  const uint32_t guess = (uint32_t)((double)n / mean_accept(sig));
+  k_walk<<<(nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, R, tiles, calls, n, guess, nstreams, cstart,
+                                            d_status);
+  k_scatter<<<dim3(calls, nstreams), 256, 0, s>>>(cand, amask, elocal, tsum, cstart, R, tiles, calls, n, mod_args(),
+                                                  d_out);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npolys, uint32_t n, uint32_t *d_out,
+                   uint32_t *d_status, cudaStream_t s) {
+  const uint32_t threads = npolys * (n / 8);
+  const uint32_t grid = (threads + 255) / 256;
+  const double kinv = kinv_of(sig);
+  if (sig == 0)
+    k_gauss_gpu_map<0><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+  else if (sig == 1)
+    k_gauss_gpu_map<1><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+  else
+    k_gauss_gpu_map<2><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+int sample_polya(const uint32_t *d_rkey, uint32_t n, uint32_t *d_a, cudaStream_t s) {
+  const uint32_t grid = (n / 2 + 255) / 256;
+  k_polya<<<grid, 256, kAesSmemBytes, s>>>(d_rkey, n, mod_args(), d_a);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+}  // namespace cufe

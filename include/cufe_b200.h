@@ -1,0 +1,152 @@
+/*
+ * cufe_b200.h -- C ABI of cufe_b200, a B200-native (sm_100a) implementation of cuFE's
+ * RLWE inner-product functional-encryption path.
+ *
+ * Two layers:
+ *   1. Drop-in symbols with the exact names and argument lists of the reference's GPU
+ *      entry points (cuFE src/rlwe_sife_gpu.cu, PERF build), bound by the reference's own
+ *      callers (src/rlwe_sife.c:23-29 and main.c:22-28).  Host buffers, synchronous,
+ *      reference layouts and the reference GPU counter-to-sample mapping.
+ *   2. A context API with runtime ring degree n and vector length l, device pointers and
+ *      stream ordering, covering both randomness mappings (the reference CPU path's streams,
+ *      bit-exact with svm_predict3, and the GPU kernels' counter mapping), batched
+ *      encryption, multi-key keygen, cross-product decryption and on-device decode.
+ *
+ * Layouts (src/rlwe_sife.h:10-26): mpk[l+1][3][n] with NTT(a) at index l, msk[l][3][n],
+ * ct[l+1][3][n] with c_0 at index l, sk_y[3][n], d_y[3][n], x and y uint32[l]; all residues
+ * are canonical in [0, q_j).  The three RNS primes are those of src/params.h:19.
+ */
+#ifndef CUFE_B200_H
+#define CUFE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference returns void and checks nothing) */
+#define CUFE_OK 0
+#define CUFE_ERR_INVALID (-1)     /* bad argument or unsupported size */
+#define CUFE_ERR_CUDA (-2)        /* CUDA runtime error; text in cufe_last_error() */
+#define CUFE_ERR_NOMEM (-3)       /* device allocation failed */
+#define CUFE_ERR_SAMPLER (-4)     /* sampler status word set; outputs of that call are invalid */
+#define CUFE_ERR_NODEVICE (-5)    /* no CUDA device */
+
+/* sampler index: sigma_1 (setup), sigma_2 (r, f_0), sigma_3 (f_i) (src/gauss.c:11-13) */
+#define CUFE_SIGMA1 0
+#define CUFE_SIGMA2 1
+#define CUFE_SIGMA3 2
+
+const char *cufe_last_error(void);
+const char *cufe_version(void);
+
+/* =====================================================================================
+ * 1. Reference drop-in.  Dimensions: those set by cufe_dropin_configure (default n = 4096,
+ *    l = 785, the values of src/params.h:21-22).  Failures leave outputs untouched, print
+ *    one line to stderr and are reported by cufe_dropin_status().
+ * ===================================================================================== */
+
+/* replaces rlwe_sife_setup_gpu (src/rlwe_sife_gpu.cu:19); mpk[l] holds a (coefficient domain)
+ * on entry; s_i from seed2, e_i from seed3, GPU counter mapping */
+void rlwe_sife_setup_gpu(uint32_t *mpk, uint32_t *msk, unsigned char *seed2, unsigned char *seed3,
+                         float *part2_time);
+/* replaces rlwe_sife_encrypt_gpu (src/rlwe_sife_gpu.cu:102); m[repeat][l], c[repeat][l+1][3][n];
+ * every instance draws r, f_0 and f_i from seed2 as the reference kernels do (seed3 unused) */
+void rlwe_sife_encrypt_gpu(uint32_t *m, uint32_t *mpk, uint32_t *c, unsigned char *seed2,
+                           unsigned char *seed3, int repeat, float *part2_time);
+/* replaces rlwe_sife_keygen_gpu (src/rlwe_sife_gpu.cu:191); y[repeat][l] -> sk_y[repeat][3][n] */
+void rlwe_sife_keygen_gpu(const uint32_t *y, const uint32_t *msk, uint32_t *sk_y, int repeat,
+                          float *part2_time);
+/* replaces rlwe_sife_decrypt_gmp_gpu (src/rlwe_sife_gpu.cu:231); one ciphertext, repeat keys
+ * -> d_y[repeat][3][n] residues (undecoded, as the reference) */
+void rlwe_sife_decrypt_gmp_gpu(uint32_t *c, const uint32_t *y, uint32_t *sk_y, uint32_t *d_y, int repeat,
+                               float *part2_time);
+
+int cufe_dropin_configure(int n, int l, int device);
+int cufe_dropin_status(void);
+
+/* =====================================================================================
+ * 2. Context API.  Every call is asynchronous and ordered on the `stream` argument
+ *    (a cudaStream_t; NULL is the legacy default stream).  Seeds and keys are host pointers
+ *    and are consumed before the call returns.
+ * ===================================================================================== */
+
+typedef struct cufe_ctx cufe_ctx;
+
+/* n: power of two in [16, 8192]; l: vector length (p = 64 l + 1, Delta = floor(q/p)) */
+int cufe_create(cufe_ctx **ctx, int n, int l, int device);
+int cufe_destroy(cufe_ctx *ctx);
+/* waits for all work queued on `stream` and reports the sampler
+ * status word (CUFE_ERR_SAMPLER if any sampler call since the last check hit an undefined
+ * reference case or ran out of precomputed refills) */
+int cufe_sync(cufe_ctx *ctx, void *stream);
+/* a non-blocking stream owned by the context */
+void *cufe_ctx_stream(cufe_ctx *ctx);
+/* p and floor(q/p) mod q_j */
+int cufe_params(const cufe_ctx *ctx, uint32_t *p, uint32_t delta_mod[3]);
+/* twiddle tables [3][n] (psi^{bitrev(i)}, psi^{-bitrev(i)}) in host memory */
+int cufe_tables(const cufe_ctx *ctx, uint32_t *psi, uint32_t *psi_inv);
+
+/* setup, CPU mapping (rlwe_sife_setup, src/rlwe_sife.c:32-82): a from seed_a
+ * (sample_polya), s_i from the seed_s stream (NULL: the all-zero round-key stream of the
+ * reference CPU path), e_i from the seed_e stream.  Seeds are host pointers. */
+int cufe_setup(cufe_ctx *ctx, const uint8_t seed_a[32], const uint8_t *seed_s, const uint8_t seed_e[32],
+               uint32_t *d_mpk, uint32_t *d_msk, void *stream);
+/* setup, GPU counter mapping (rlwe_sife_setup_gpu): d_mpk[l] holds a on entry */
+int cufe_setup_gpu_map(cufe_ctx *ctx, const uint8_t seed2[32], const uint8_t seed3[32], uint32_t *d_mpk,
+                       uint32_t *d_msk, void *stream);
+
+/* batch independent encryptions, CPU mapping (rlwe_sife_encrypt, src/rlwe_sife.c:112-181):
+ * instance b draws r and f_0 from seeds2[b], f_i from seeds3[b] (seeds3 NULL: the zero-key
+ * stream of the reference CPU path).  d_x[batch][l], d_ct[batch][l+1][3][n]. */
+int cufe_encrypt(cufe_ctx *ctx, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                 const uint8_t *seeds3, uint32_t *d_ct, void *stream);
+/* GPU counter mapping (rlwe_sife_encrypt_gpu): all instances share seed2's randomness */
+int cufe_encrypt_gpu_map(cufe_ctx *ctx, int batch, const uint32_t *d_x, const uint32_t *d_mpk,
+                         const uint8_t seed2[32], uint32_t *d_ct, void *stream);
+
+/* sk_y = sum_i y_i msk_i (rlwe_sife_keygen, src/rlwe_sife.c:215-245) for nkeys vectors
+ * d_y[nkeys][l]; y_signed = 0 reduces y as uint32 (the reference), 1 as int32 */
+int cufe_keygen(cufe_ctx *ctx, int nkeys, const uint32_t *d_y, int y_signed, const uint32_t *d_msk,
+                uint32_t *d_sky, void *stream);
+/* d_y = sum_i y_i c_i - c_l * sk_y (rlwe_sife_decrypt_gmp before the CRT,
+ * src/rlwe_sife.c:248-278) for every (ciphertext, key) pair: d_dy[nct][nkeys][3][n] */
+int cufe_decrypt(cufe_ctx *ctx, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                 const uint32_t *d_sky, uint32_t *d_dy, void *stream);
+/* crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332) on the first
+ * ncoeff coefficients of each of count d_y: d_out[count][ncoeff], values in [0, p] */
+int cufe_decode(cufe_ctx *ctx, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, void *stream);
+
+/* samplers, for parity tests and statistics.  CPU mapping: nstreams AES-CTR streams keyed by
+ * keys[nstreams][32] (NULL: zero-key streams), each running `calls` consecutive
+ * gaussian_sampler_S* calls of n samples (src/gauss.c:789,995,1086): d_out[nstreams][calls][3][n]. */
+int cufe_sample_cpu_map(cufe_ctx *ctx, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
+                        void *stream);
+/* GPU counter mapping (src/sample_gpu.cu:40-289) for polynomials poly0..poly0+npolys-1 */
+int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0, int npolys, uint32_t *d_out,
+                        void *stream);
+/* sample_polya (src/sample.c:56-128): d_a[3][n] */
+int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void *stream);
+
+/* =====================================================================================
+ * 3. Negacyclic NTT on an RNS ring (CT_forward / GS_reverse, src/ntt.c:38-114)
+ * ===================================================================================== */
+
+typedef struct cufe_ring cufe_ring;
+
+/* k primes (NULL: the params.h primes, then the largest primes below 2^31 that are 1 mod
+ * 2^14); n power of two in [16, 8192], k in [1, 6] */
+int cufe_ring_create(cufe_ring **ring, int n, int k, const uint32_t *primes, int device);
+int cufe_ring_destroy(cufe_ring *ring);
+/* primes[k], roots[k] (the primitive 2n-th roots used), tables [k][n] */
+int cufe_ring_info(const cufe_ring *ring, uint32_t *primes, uint32_t *roots, uint32_t *psi, uint32_t *psi_inv);
+/* in place on d_data[npoly][k][n]; forward: natural -> bit-reversed order */
+int cufe_ntt_forward(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
+int cufe_ntt_inverse(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

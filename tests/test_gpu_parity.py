@@ -1,0 +1,197 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, on a GPU.
+
+The oracle (oracle/cufe_oracle.c) is pinned bit-for-bit to the reference's own CPU build
+(tests/test_oracle.py); residues are compared canonically (the reference's mod_prime may
+return q_j for 0).
+"""
+import numpy as np
+import pytest
+
+from oracle.ffi import Oracle, canon, aes256_expand
+from tests.conftest import seeds
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+import cufe_b200 as cf  # noqa: E402
+
+
+def dev(a):
+    return cf.to_dev(a)
+
+
+@pytest.fixture(scope="module")
+def ctx_small(oracle_built):
+    c = cf.Context(256, 8)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("n", [16, 64, 256, 1024, 2048, 4096, 8192])
+@pytest.mark.parametrize("k", [3, 6])
+def test_ntt_roundtrip_and_values(n, k, rng, oracle_built):
+    ring = cf.Ring(n, k)
+    npoly = 5
+    q = ring.primes.astype(np.uint64)
+    a = (rng.integers(0, 2**31, (npoly, k, n), dtype=np.uint64) % q[None, :, None]).astype(np.uint32)
+    d = dev(a)
+    ring.forward(d)
+    got = cf.u32(d)
+    O = Oracle.lib()
+    for p in range(npoly):
+        for m in range(k):
+            ref = a[p, m].copy()
+            O.or_ntt_generic(ref, n, int(q[m]), np.ascontiguousarray(ring.psi[m]), 0, 0)
+            assert (got[p, m] == ref).all(), (n, k, p, m)
+    ring.inverse(d)
+    assert (cf.u32(d) == a).all()
+
+
+def test_ntt_tables_match_reference_chain(oracle_built):
+    # the params.h primes use the reference twiddle chain (consts.h), checked via the oracle
+    for n in (256, 4096):
+        ring = cf.Ring(n, 3)
+        t = Oracle(n, 1).tables()
+        assert (ring.psi == t["psi"]).all() and (ring.psi_inv == t["psi_inv"]).all()
+
+
+def test_sample_polya(ctx_small, rng):
+    s = seeds(rng)[0]
+    got = cf.u32(ctx_small.sample_polya(s))
+    torch.cuda.synchronize()
+    assert (got == Oracle(256, 8).sample_polya(s)).all()
+
+
+@pytest.mark.parametrize("sig", [0, 1, 2])
+def test_sampler_cpu_map(sig, rng, oracle_built):
+    n = 1024
+    c = cf.Context(n, 4)
+    keys = seeds(rng, 3)
+    calls = 5
+    got = cf.u32(c.sample_cpu_map(sig, keys, calls))
+    zero = cf.u32(c.sample_cpu_map(sig, None, calls, nstreams=2))
+    c.sync()
+    O = Oracle(n, 4)
+    for i in range(3):
+        ref, _ = O.gauss(sig, keys[i], calls)
+        assert (got[i] == canon(ref)).all(), (sig, i)
+    ref, _ = O.gauss(sig, None, calls)
+    assert (zero[0] == canon(ref)).all() and (zero[1] == canon(ref)).all()
+
+
+@pytest.mark.parametrize("sig", [0, 1, 2])
+def test_sampler_gpu_map(sig, rng, oracle_built):
+    n = 4096
+    c = cf.Context(n, 4)
+    key = seeds(rng)[0]
+    got = cf.u32(c.sample_gpu_map(sig, key, 2, 3))
+    c.sync()
+    O = Oracle(n, 4)
+    rk = aes256_expand(key)
+    for p in range(3):
+        assert (got[p] == canon(O.gauss_modeB(rk, sig, 2 + p))).all(), (sig, p)
+
+
+@pytest.mark.parametrize("n,l", [(256, 8), (1024, 16), (2048, 124)])
+def test_scheme_cpu_map(n, l, rng, oracle_built):
+    c = cf.Context(n, l)
+    O = Oracle(n, l)
+    sa, se, ss = seeds(rng, 3)
+    mpk, msk = c.setup(sa, None, se)
+    rmpk, rmsk = O.setup(sa, None, se)
+    assert (cf.u32(mpk) == canon(rmpk)).all()
+    assert (cf.u32(msk) == canon(rmsk)).all()
+    # seeded secret stream too
+    mpk2, msk2 = c.setup(sa, ss, se)
+    r2mpk, r2msk = O.setup(sa, ss, se)
+    assert (cf.u32(mpk2) == canon(r2mpk)).all() and (cf.u32(msk2) == canon(r2msk)).all()
+    B = 3
+    x = rng.integers(0, 5, (B, l), dtype=np.uint32)
+    s2 = seeds(rng, B)
+    s3 = seeds(rng, B)
+    ct = c.encrypt(dev(x), mpk, s2, None)
+    ct3 = c.encrypt(dev(x), mpk, s2, s3)
+    got, got3 = cf.u32(ct), cf.u32(ct3)
+    y = rng.integers(0, 17, (2, l), dtype=np.uint32)
+    sky = c.keygen(dev(y), msk)
+    gsky = cf.u32(sky)
+    dy = c.decrypt(ct, dev(y), sky)
+    gdy = cf.u32(dy)
+    dec = cf.u32(c.decode(dy))
+    c.sync()
+    for b in range(B):
+        rct = O.encrypt(x[b], rmpk, s2[b], None)
+        assert (got[b] == canon(rct)).all(), ("ct", b)
+        assert (got3[b] == canon(O.encrypt(x[b], rmpk, s2[b], s3[b]))).all(), ("ct3", b)
+        for k in range(2):
+            rsk = O.keygen(y[k], rmsk)
+            if b == 0:
+                assert (gsky[k] == canon(rsk)).all()
+            rdy = O.decrypt(rct, y[k], rsk)
+            assert (gdy[b, k] == canon(rdy)).all(), ("dy", b, k)
+            rdec = O.decode(rdy)
+            assert (dec[b * 2 + k] == rdec).all()
+            assert int(rdec[0]) == int(x[b].astype(np.int64) @ y[k].astype(np.int64))
+
+
+def test_scheme_gpu_map(rng, oracle_built):
+    n, l = 1024, 16
+    c = cf.Context(n, l)
+    O = Oracle(n, l)
+    a = O.sample_polya(seeds(rng)[0])
+    s2, s3 = seeds(rng, 2)
+    mpk, msk = c.setup_gpu_map(dev(a), s2, s3)
+    rmpk, rmsk = O.setup_modeB(a, s2, s3)
+    assert (cf.u32(mpk) == canon(rmpk)).all() and (cf.u32(msk) == canon(rmsk)).all()
+    x = rng.integers(0, 5, (3, l), dtype=np.uint32)
+    ct = cf.u32(c.encrypt_gpu_map(dev(x), mpk, s2))
+    c.sync()
+    assert (ct == canon(O.encrypt_modeB(x, rmpk, s2))).all()
+
+
+def test_decode_random_residues(ctx_small, rng):
+    n = 256
+    q = np.array(cf.Q, np.uint64)
+    dy = (rng.integers(0, 2**62, (4, 3, n), dtype=np.uint64) % q[None, :, None]).astype(np.uint32)
+    got = cf.u32(ctx_small.decode(dev(dy)))
+    ctx_small.sync()
+    O = Oracle(n, 8)
+    for i in range(4):
+        assert (got[i] == O.decode(dy[i])).all()
+
+
+def test_dropin_abi(rng, oracle_built):
+    """the reference's four GPU symbols, host buffers, GPU counter mapping"""
+    import ctypes as C
+    n, l = 1024, 16
+    L = cf.lib()
+    assert L.cufe_dropin_configure(n, l, 0) == 0
+    O = Oracle(n, l)
+    s2, s3 = seeds(rng, 2)
+    mpk = np.zeros((l + 1, 3, n), np.uint32)
+    msk = np.zeros((l, 3, n), np.uint32)
+    mpk[l] = O.sample_polya(seeds(rng)[0])
+    a = mpk[l].copy()
+    t = C.c_float(0)
+    L.rlwe_sife_setup_gpu(mpk.ctypes.data, msk.ctypes.data, s2.ctypes.data, s3.ctypes.data, C.byref(t))
+    assert L.cufe_dropin_status() == 0
+    rmpk, rmsk = O.setup_modeB(a, s2, s3)
+    assert (mpk == canon(rmpk)).all() and (msk == canon(rmsk)).all()
+    assert t.value > 0
+    rep = 2
+    x = rng.integers(0, 5, (rep, l), dtype=np.uint32)
+    ct = np.zeros((rep, l + 1, 3, n), np.uint32)
+    L.rlwe_sife_encrypt_gpu(x.ctypes.data, mpk.ctypes.data, ct.ctypes.data, s2.ctypes.data, s2.ctypes.data, rep, None)
+    assert (ct == canon(O.encrypt_modeB(x, rmpk, s2))).all()
+    y = rng.integers(0, 17, (3, l), dtype=np.uint32)
+    sk = np.zeros((3, 3, n), np.uint32)
+    L.rlwe_sife_keygen_gpu(y.ctypes.data, msk.ctypes.data, sk.ctypes.data, 3, None)
+    dy = np.zeros((3, 3, n), np.uint32)
+    L.rlwe_sife_decrypt_gmp_gpu(ct[0].ctypes.data, y.ctypes.data, sk.ctypes.data, dy.ctypes.data, 3, None)
+    assert L.cufe_dropin_status() == 0
+    for k in range(3):
+        rsk = O.keygen(y[k], rmsk)
+        assert (sk[k] == canon(rsk)).all()
+        rdy = O.decrypt(ct[0], y[k], rsk)
+        assert (dy[k] == canon(rdy)).all()
+        assert int(O.decode(rdy)[0]) == int(x[0].astype(np.int64) @ y[k].astype(np.int64))
