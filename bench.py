@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""bench.py -- IPFE inner products/sec at N=4096 (bit-exact), batched vs plain GPU; p99 ms.
+
+Workload (the reference's plain GPU pipeline shape): ring N = 4096, the three params.h RNS
+primes, l = 784 (p = 50177), x uniform in [0, 4], y uniform in [-16, 16], 10,000 encryptions
+x 1 function key, seeded synthetic data (SplitMix-style numpy seeds).  One inner product =
+encrypt(x) + keygen(y) (one key, done once) + decrypt + decode of all N coefficients; the
+inner product is coefficient 0, centred.  A step is one batch of B encryptions through the
+whole pipeline; the batch output is checked against the plaintext dot products after timing.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl cufe|reference]
+
+--impl reference times the reference's own CPU implementation (cuFE src/*.c compiled from
+source, oracle/_ref) on this host's cores, one process per core.  Under torchrun each rank
+drives its own GPU with an independent replica of the workload (the path has no exchange
+step); the value is all ranks' inner products over the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N, L = 4096, 784
+TOTAL_ENC = 10000
+METRIC = "IPFE inner products/sec at N=4096 (bit-exact), batched vs plain GPU; p99 ms"
+UNIT = "IP/s"
+SEED = 0xC0FE0002
+
+
+def workload():
+    rng = np.random.default_rng(SEED)
+    x = rng.integers(0, 5, (TOTAL_ENC, L), dtype=np.uint32)
+    y = rng.integers(-16, 17, (1, L), dtype=np.int32)
+    seeds2 = rng.integers(0, 256, (TOTAL_ENC, 32), dtype=np.uint8)
+    seeds3 = rng.integers(0, 256, (TOTAL_ENC, 32), dtype=np.uint8)
+    setup_seeds = rng.integers(0, 256, (3, 32), dtype=np.uint8)
+    return x, y, seeds2, seeds3, setup_seeds
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class Clocks:
+    def __init__(self, device, out):
+        self.out = out
+        self.p = None
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(device), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(out, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        rows = []
+        for line in open(self.out):
+            f = [t.strip() for t in line.split(",")]
+            if len(f) >= 7:
+                try:
+                    rows.append((float(f[0]), float(f[1]), f[3:7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def _ref_worker_init(path):
+    global _REF, _REFDATA
+    from oracle.ffi import Reference
+    _REF = Reference("n4096_l784")
+    d = np.load(path)
+    _REFDATA = {k: d[k] for k in d.files}
+
+
+def _ref_one(i):
+    """one inner product on the reference CPU path: encrypt + two decrypts (signed y split
+    into y+ - y-, since the reference reduces y as uint32) with their GMP decode"""
+    d = _REFDATA
+    ct = _REF.encrypt(d["x"][i], d["mpk"], d["s2"][i])
+    _, dp = _REF.decrypt(ct, d["yp"], d["skp"])
+    _, dm = _REF.decrypt(ct, d["ym"], d["skm"])
+    p = 64 * L + 1
+
+    def centred(v):
+        v = int(v) % p
+        return v - p if v > p // 2 else v
+    return centred(int(dp[0]) - int(dm[0]))
+
+
+def reference_pool(x, y, seeds2, setup_seeds, nproc):
+    """spawned processes with the reference CPU build; keys made once by the reference setup"""
+    import multiprocessing as mp
+    from oracle.ffi import Reference
+    R = Reference("n4096_l784")
+    mpk, msk = R.setup(setup_seeds[0], setup_seeds[2])
+    yv = y[0].astype(np.int64)
+    yp = np.where(yv > 0, yv, 0).astype(np.uint32)
+    ym = np.where(yv < 0, -yv, 0).astype(np.uint32)
+    skp, skm = R.keygen(yp, msk), R.keygen(ym, msk)
+    tmp = tempfile.NamedTemporaryFile(suffix=".npz", delete=False)
+    np.savez(tmp.name, x=x, mpk=mpk, s2=seeds2, yp=yp, ym=ym, skp=skp, skm=skm)
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(nproc, initializer=_ref_worker_init, initargs=(tmp.name,))
+    return pool, tmp.name
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    x, y, seeds2, _, setup_seeds = workload()
+    nproc = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    pool, path = reference_pool(x, y, seeds2, setup_seeds, nproc)
+    try:
+        idx = 0
+        times = []
+        ok = True
+        for step in range(args.warmup + args.steps):
+            ids = [(idx + j) % TOTAL_ENC for j in range(nproc)]
+            idx += nproc
+            t0 = time.perf_counter()
+            res = pool.map(_ref_one, ids)
+            dt = time.perf_counter() - t0
+            exp = [int(x[i].astype(np.int64) @ y[0].astype(np.int64)) for i in ids]
+            ok = ok and res == exp
+            if step >= args.warmup:
+                times.append(dt)
+    finally:
+        pool.terminate()
+        os.unlink(path)
+    total = sum(times)
+    value = nproc * len(times) / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint32",
+            "data": "synthetic", "bit_exact": ok,
+            "config": {"workload": "N=4096 l=784, x in [0,4], y in [-16,16], 10000 encryptions x 1 key",
+                       "n": N, "l": L, "step": "%d inner products, one per process" % nproc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference",
+                             "sample": "%d steps x %d processes, 1 inner product each (encrypt + "
+                                       "2 decrypts for signed y + GMP decode)" % (args.steps, nproc)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample(x, y, seeds2, setup_seeds, nproc, steps=2):
+    pool, path = reference_pool(x, y, seeds2, setup_seeds, nproc)
+    try:
+        pool.map(_ref_one, list(range(nproc)))  # warm
+        t0 = time.perf_counter()
+        for s in range(steps):
+            pool.map(_ref_one, [(nproc * (s + 1) + j) % TOTAL_ENC for j in range(nproc)])
+        dt = time.perf_counter() - t0
+    finally:
+        pool.terminate()
+        os.unlink(path)
+    return {"value": nproc * steps / dt, "unit": UNIT, "cores": nproc, "kind": "reference",
+            "sample": "%d rounds x %d processes, 1 inner product each (reference CPU build, "
+                      "encrypt + 2 decrypts for signed y + GMP decode)" % (steps, nproc)}
+
+
+# ----------------------------------------------------------------------------- GPU arm
+
+# algorithmic HBM bytes per launch of each kernel at this workload (batch B)
+def algorithmic_bytes(kernel, B, refills3):
+    poly = 3 * N * 4
+    return {
+        "sample_cand_s3": refills3 * B * 65,           # 8 x int64 candidates + accept mask
+        "sample_scatter": refills3 * B * 69 + B * L * poly,  # candidates, masks, prefixes; f_i residues
+        "encrypt_intt": (L + 1) * poly + B * (L * poly + (L + 1) * poly),  # mpk once, f_i, ciphertexts
+        "decrypt": B * (L + 1) * poly + B * poly,        # ciphertexts read, d_y written
+        "decode": B * poly + B * N * 4,
+    }.get(kernel)
+
+
+def gpu_arm(args):
+    import torch
+    import cufe_b200 as cf
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = "cuda:%d" % local
+    x, y, seeds2, seeds3, setup_seeds = workload()
+    B = args.batch
+    nb = TOTAL_ENC // B
+    ctx = cf.Context(N, L, device=local)
+    mpk, msk = ctx.setup(setup_seeds[0], setup_seeds[1], setup_seeds[2])
+    y_dev = torch.from_numpy(y.copy()).to(dev)
+    sky = ctx.keygen(y_dev, msk, y_signed=True)
+    x_dev = cf.to_dev(x, dev)
+    ct = ctx.ct_buf(B)
+    dy = torch.empty((B, 1, 3, N), dtype=torch.int32, device=dev)
+    steps, warm = args.steps, args.warmup
+    res = torch.empty((steps, B, N), dtype=torch.int32, device=dev)
+    scratch = torch.empty((B, N), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(local)
+
+    def step(k, out):
+        b0 = (k % nb) * B
+        ctx.encrypt(x_dev[b0:b0 + B], mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
+        ctx.decrypt(ct, y_dev, sky, y_signed=True, dy=dy)
+        ctx.decode(dy, out=out)
+
+    for w in range(warm):
+        step(w, scratch)
+    ctx.sync()
+
+    # --- batched, device-resident inputs (value)
+    clk = Clocks(local, os.path.join(tempfile.gettempdir(), "cufe_clocks_%d.csv" % rank))
+    ctx.profile_reset()
+    ctx.profile(True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    e0.record(stream)
+    step_ev[0].record(stream)
+    for k in range(steps):
+        step(warm + k, res[k])
+        step_ev[k + 1].record(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = clk.stop()
+    ctx.profile(False)
+    prof = ctx.profile_read()
+    ctx.sync()
+    step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(steps)]
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    # correctness of every inner product in the timed region
+    got = cf.u32(res[:, :, 0]).astype(np.int64)
+    p = ctx.p
+    got = np.where(got > p // 2, got - p, got)
+    ids = np.array([((warm + k) % nb) * B + j for k in range(steps) for j in range(B)]).reshape(steps, B)
+    exp = x[ids].astype(np.int64) @ y[0].astype(np.int64)
+    bit_exact = bool((got == exp).all())
+    ips = steps * B * world / (ms / 1000.0)
+
+    # --- plain per-call form: one encryption per call, synchronised each call
+    nplain = args.plain_calls
+    pl_ct = ctx.ct_buf(1)
+    pl_dy = torch.empty((1, 1, 3, N), dtype=torch.int32, device=dev)
+    pl_out = torch.empty((1, N), dtype=torch.int32, device=dev)
+    lat = []
+    for i in range(nplain + 2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.encrypt(x_dev[i:i + 1], mpk, seeds2[i:i + 1], seeds3[i:i + 1], ct=pl_ct)
+        ctx.decrypt(pl_ct, y_dev, sky, y_signed=True, dy=pl_dy)
+        ctx.decode(pl_dy, out=pl_out)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            lat.append(a.elapsed_time(b))
+    plain = {"value": 1000.0 * len(lat) / sum(lat), "unit": UNIT, "calls": len(lat),
+             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+             "form": "one encryption per call (batch 1), device-resident, same kernels"}
+
+    # --- end to end through the C ABI with host buffers (pinned), copies in the timed region
+    xh = torch.from_numpy(x.view(np.int32)).pin_memory()
+    rh = torch.empty((steps, B), dtype=torch.int32).pin_memory()
+    xd = torch.empty((B, L), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for k in range(steps):
+        b0 = ((warm + k) % nb) * B
+        xd.copy_(xh[b0:b0 + B], non_blocking=True)
+        ctx.encrypt(xd, mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
+        ctx.decrypt(ct, y_dev, sky, y_signed=True, dy=dy)
+        ctx.decode(dy, out=scratch)
+        rh[k].copy_(scratch[:, 0], non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_ok = bool((np.where(rh.numpy().view(np.uint32).astype(np.int64) > p // 2,
+                            rh.numpy().view(np.uint32).astype(np.int64) - p,
+                            rh.numpy().view(np.uint32).astype(np.int64)) == exp).all())
+    e2e = {"value": steps * B * world / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": B * L * 4 + B * 64, "d2h_bytes_per_step": B * 4, "bit_exact": e2e_ok}
+
+    # --- roofline of the dominant kernel (device time summed over the timed region)
+    from cufe_b200 import _refills_s3
+    refills3 = _refills_s3(N, L)
+    launches = sum(v[0] for v in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (cnt, tot) = dom
+    per_launch_s = tot / cnt / 1000.0
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    abytes = algorithmic_bytes(name, B, refills3)
+    roof = {"kernel": name, "bound": "hbm", "unit": "GB/s", "peak": hbm_peak,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "achieved": (abytes / per_launch_s / 1e9) if abytes else None, "traffic": None,
+            "share": tot / sum(v[1] for v in prof.values())}
+    roof["frac"] = roof["achieved"] / hbm_peak if roof["achieved"] else None
+    if name.startswith("sample_cand"):
+        # the AES keystream bounds this kernel: 15 AES-256 blocks per refill, each
+        # 14 rounds x 16 T-table lookups from shared memory (one warp LDS per clock per SM)
+        blocks = refills3 * B * 15
+        sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        lds_peak = 148 * sm_mhz * 1e6 * 32 / (14 * 16)
+        roof["pipe"] = {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)",
+                        "achieved": blocks / per_launch_s, "peak_lds_bound": lds_peak,
+                        "frac": blocks / per_launch_s / lds_peak, "sm_mhz": sm_mhz}
+
+    line = {"metric": METRIC, "value": ips, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "uint32", "data": "synthetic", "bit_exact": bit_exact,
+            "config": {"workload": "N=4096 l=784, x in [0,4], y in [-16,16], 10000 encryptions x 1 key "
+                                   "(plain GPU pipeline shape), batched",
+                       "n": N, "l": L, "batch": B, "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (a batch of ciphertexts is %.1f GB)" % (B * (L + 1) * 3 * N * 4 / 1e9),
+                       "randomness": "CPU stream mapping, every stream keyed by a per-encryption seed"},
+            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+            "plain": plain, "batched_vs_plain": ips / world / plain["value"],
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+            "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_sample(x, y, seeds2, setup_seeds,
+                                                       max(1, min(os.cpu_count() or 1, args.ref_procs)))
+        except Exception as e:  # reported, never silently replaced
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0 if bit_exact else 1
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=200)
+    ap.add_argument("--impl", default="cufe", choices=["cufe", "reference"])
+    ap.add_argument("--plain-calls", type=int, default=30)
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -50,6 +50,9 @@ def lib():
             "cufe_sync": [vp, vp],
             "cufe_ctx_stream": [vp],
             "cufe_params": [vp, vp, vp],
+            "cufe_profile_enable": [vp, i],
+            "cufe_profile_read": [vp, i, vp, vp, vp],
+            "cufe_profile_reset": [vp],
             "cufe_tables": [vp, vp, vp],
             "cufe_setup": [vp, vp, vp, vp, vp, vp, vp],
             "cufe_setup_gpu_map": [vp, vp, vp, vp, vp, vp],
@@ -66,6 +69,7 @@ def lib():
             "cufe_ring_info": [vp, vp, vp, vp, vp],
             "cufe_ntt_forward": [vp, vp, ll, vp],
             "cufe_ntt_inverse": [vp, vp, ll, vp],
+            "cufe_sampler_refills": [i, i, i],
             "cufe_dropin_configure": [i, i, i],
             "cufe_dropin_status": [],
             "rlwe_sife_setup_gpu": [vp, vp, vp, vp, vp],
@@ -77,8 +81,14 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = None if name.startswith("rlwe_sife_") else C.c_int
+        L.cufe_sampler_refills.restype = C.c_longlong
         _lib = L
     return _lib
+
+
+def _refills_s3(n, l):
+    """refills per encryption stream of the sigma_3 sampler (CPU mapping)"""
+    return int(lib().cufe_sampler_refills(SIGMA3, l, n))
 
 
 def _check(rc, what):
@@ -158,6 +168,23 @@ class Context:
 
     def sync(self, stream=None):
         _check(lib().cufe_sync(self.h, _stream(stream, self.device)), "cufe_sync")
+
+    def profile(self, on=True):
+        _check(lib().cufe_profile_enable(self.h, int(on)), "cufe_profile_enable")
+
+    def profile_reset(self):
+        _check(lib().cufe_profile_reset(self.h), "cufe_profile_reset")
+
+    def profile_read(self):
+        """{kernel name: (launches, total ms)} since the last reset"""
+        names = C.create_string_buffer(64 * 64)
+        launches = np.zeros(64, np.int64)
+        ms = np.zeros(64, np.float64)
+        k = lib().cufe_profile_read(self.h, 64, names, launches.ctypes.data, ms.ctypes.data)
+        if k < 0:
+            raise CufeError(k, "cufe_profile_read")
+        raw = names.raw
+        return {raw[64 * i:64 * i + 64].split(b"\0")[0].decode(): (int(launches[i]), float(ms[i])) for i in range(k)}
 
     def tables(self):
         psi = np.zeros((3, self.n), np.uint32)

@@ -8,8 +8,10 @@
 #include <string>
 
 #include "ctx.h"
+#include "sampler_host.h"
 
 namespace cufe {
+thread_local Prof *t_prof = nullptr;
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 }  // namespace cufe
@@ -72,15 +74,60 @@ int cufe_destroy(cufe_ctx *h) {
 
 void *cufe_ctx_stream(cufe_ctx *h) { return h ? (void *)h->c.stream : nullptr; }
 
+struct ProfBind {
+  explicit ProfBind(cufe::Prof *p) { cufe::t_prof = p; }
+  ~ProfBind() { cufe::t_prof = nullptr; }
+};
+
 #define CTX_CALL(h, expr)                        \
   do {                                           \
     if (!(h)) return CUFE_ERR_INVALID;           \
     std::lock_guard<std::mutex> lk((h)->c.mu);   \
+    ProfBind pb(&(h)->c.prof);                   \
     if (cudaSetDevice((h)->c.device) != cudaSuccess) return CUFE_ERR_CUDA; \
     return (expr);                               \
   } while (0)
 
 int cufe_sync(cufe_ctx *h, void *stream) { CTX_CALL(h, h->c.check_status(h->c.pick(stream))); }
+
+int cufe_profile_enable(cufe_ctx *h, int on) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(h->c.mu);
+  h->c.prof.collect();
+  h->c.prof.on = on != 0;
+  return CUFE_OK;
+}
+
+int cufe_profile_read(cufe_ctx *h, int max_kernels, char *names, long long *launches, double *ms) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(h->c.mu);
+  h->c.prof.collect();
+  int i = 0;
+  for (auto &kv : h->c.prof.acc) {
+    if (i >= max_kernels) break;
+    if (names) {
+      std::strncpy(names + 64 * (size_t)i, kv.first.c_str(), 63);
+      names[64 * (size_t)i + 63] = 0;
+    }
+    if (launches) launches[i] = kv.second.first;
+    if (ms) ms[i] = kv.second.second;
+    ++i;
+  }
+  return i;
+}
+
+int cufe_profile_reset(cufe_ctx *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(h->c.mu);
+  h->c.prof.collect();
+  h->c.prof.acc.clear();
+  return CUFE_OK;
+}
+
+long long cufe_sampler_refills(int sig, int calls, int n) {
+  if (sig < 0 || sig > 2 || calls < 1 || n < 16) return -1;
+  return (long long)cufe::cpu_map_refills((uint32_t)calls, (uint32_t)n, sig);
+}
 
 int cufe_params(const cufe_ctx *h, uint32_t *p, uint32_t delta_mod[3]) {
   if (!h) return CUFE_ERR_INVALID;

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "cufe_internal.cuh"
+#include "prof.h"
 
 namespace cufe {
 
@@ -42,6 +43,7 @@ struct Ctx {
   size_t ws_bytes = 0;
   uint32_t *d_status = nullptr;  // sampler status word (device)
   std::mutex mu;                 // serialises host calls on this context
+  Prof prof;                     // per-kernel timing (cufe_profile_*)
 
   int init(int n, int l, int device);
   void release();

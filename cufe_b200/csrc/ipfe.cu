@@ -11,6 +11,7 @@
 #include "ctx.h"
 #include "ntt.cuh"
 #include "sampler_host.h"
+#include "prof.h"
 
 namespace cufe {
 
@@ -238,6 +239,7 @@ int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nre
   }
   const long long grid = (nres + G - 1) / G;
   if (grid <= 0) return CUFE_OK;
+  ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
   k_ntt<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
@@ -385,54 +387,83 @@ __global__ void __launch_bounds__(256) k_keygen(const uint32_t *__restrict__ y, 
     if (k0 + kk < nkeys) sky[((size_t)(k0 + kk) * 3 + m) * n + j] = mod_u64(acc[kk], sa.mu[m], q);
 }
 
-// d_y for ciphertext c and key k, residue m (src/rlwe_sife.c:248-278):
-// sum_i y_i c_i - INTT(NTT(c_l) NTT(sk_y)); one residue polynomial per thread group.
+// Decryption (src/rlwe_sife.c:248-278), d_y = sum_i y_i c_i - INTT(NTT(c_l) NTT(sk_y)), in
+// two kernels.  k_dec_mac streams the ciphertexts: thread = 4 consecutive coefficients of one
+// (ciphertext, key, residue), 16-byte loads, Shoup products accumulated in 64 bits; the
+// l-sum is optionally split into S chunks (small batches) with canonical partial sums.
+// k_dec_tail adds the chunks and subtracts the negacyclic product c_l * sk_y.
+__global__ void __launch_bounds__(256) k_dec_mac(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ y,
+                                                 int y_signed, int nkeys, int nsplit, uint32_t *__restrict__ part,
+                                                 SchemeArgs sa) {
+  extern __shared__ uint32_t smem_u32[];
+  const int n = sa.ra.n, l = sa.l;
+  const int per_poly = n / 4 / blockDim.x;  // CTAs per residue polynomial
+  const int s = blockIdx.x / per_poly, sub = blockIdx.x - s * per_poly;
+  const int w = blockIdx.y;  // (c * nkeys + key) * 3 + m
+  const int m = w % 3, ck = w / 3, key = ck % nkeys, c = ck / nkeys;
+  const uint32_t q = sa.ra.q[m];
+  const int i0 = (int)((long long)l * s / nsplit), i1 = (int)((long long)l * (s + 1) / nsplit);
+  uint32_t *yq = smem_u32, *ys = smem_u32 + (i1 - i0);
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const uint32_t v = y_residue(y[(size_t)key * l + i], y_signed, q, sa.mu[m]);
+    yq[i - i0] = v;
+    ys[i - i0] = (uint32_t)(((uint64_t)v << 32) / q);
+  }
+  __syncthreads();
+  const int j = 4 * (sub * blockDim.x + threadIdx.x);
+  const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * n + (size_t)m * n + j;
+  uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll 4
+  for (int i = i0; i < i1; ++i) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(cb + (size_t)i * 3 * n));
+    const uint32_t yv = yq[i - i0], yh = ys[i - i0];
+    a0 += shoup_lazy(v.x, yv, yh, q);
+    a1 += shoup_lazy(v.y, yv, yh, q);
+    a2 += shoup_lazy(v.z, yv, yh, q);
+    a3 += shoup_lazy(v.w, yv, yh, q);
+  }
+  uint4 o;
+  o.x = mod_u64(a0, sa.mu[m], q);
+  o.y = mod_u64(a1, sa.mu[m], q);
+  o.z = mod_u64(a2, sa.mu[m], q);
+  o.w = mod_u64(a3, sa.mu[m], q);
+  *reinterpret_cast<uint4 *>(part + ((size_t)w * nsplit + s) * n + j) = o;
+}
+
 template <int LOGN>
 __global__ void __launch_bounds__(512)
-    k_decrypt(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ clhat, const uint32_t *__restrict__ skhat,
-              const uint32_t *__restrict__ skhat_sh, const uint32_t *__restrict__ y, int y_signed, int nct, int nkeys,
-              uint32_t *__restrict__ dy, long long nwork, SchemeArgs sa) {
+    k_dec_tail(const uint32_t *__restrict__ part, int nsplit, const uint32_t *__restrict__ clhat,
+               const uint32_t *__restrict__ skhat, const uint32_t *__restrict__ skhat_sh, int nkeys,
+               uint32_t *__restrict__ dy, long long nwork, SchemeArgs sa) {
   using P = NttPlan<LOGN>;
   extern __shared__ uint32_t smem_u32[];
-  const int th = threadIdx.x, l = sa.l;
+  const int th = threadIdx.x;
   const long long wi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
   const bool act = wi < nwork;
   const long long ww = act ? wi : nwork - 1;
-  // work index = (c * nkeys + k) * 3 + m
   const int m = (int)(ww % 3);
   const long long ck = ww / 3;
   const int key = (int)(ck % nkeys), c = (int)(ck / nkeys);
   const uint32_t q = sa.ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * (P::N + 2 * l);
-  uint32_t *yq = sm + P::N, *ys = yq + l;
-  for (int i = th; i < l; i += P::T) {
-    const uint32_t v = y_residue(y[(size_t)key * l + i], y_signed, q, sa.mu[m]);
-    yq[i] = v;
-    ys[i] = (uint32_t)(((uint64_t)v << 32) / q);
-  }
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
   uint32_t a[16], w[16], wsh[16];
   load16(clhat + ((size_t)c * 3 + m) * P::N + th * 16, a);
   load16(skhat + ((size_t)key * 3 + m) * P::N + th * 16, w);
   load16(skhat_sh + ((size_t)key * 3 + m) * P::N + th * 16, wsh);
 #pragma unroll
   for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
-  __syncthreads();
   ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi + (size_t)m * P::N, sa.ra.ipsi_sh + (size_t)m * P::N, sa.ra.ninv[m],
                      sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
-  uint64_t acc[16];
-#pragma unroll
-  for (int e = 0; e < 16; ++e) acc[e] = 0;
-  const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * P::N + (size_t)m * P::N;
-  for (int i = 0; i < l; ++i) {
-    const uint32_t yv = yq[i], yh = ys[i];
-    const uint32_t *ci = cb + (size_t)i * 3 * P::N;
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] += shoup_lazy(__ldg(ci + P::template idx<0>(th, e)), yv, yh, q);
-  }
   if (act) {
+    const uint32_t *pp = part + (size_t)ww * nsplit * P::N;
     uint32_t *o = dy + ww * P::N;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) o[P::template idx<0>(th, e)] = mod_sub(mod_u64(acc[e], sa.mu[m], q), a[e], q);
+    for (int e = 0; e < 16; ++e) {
+      const int j = P::template idx<0>(th, e);
+      uint32_t mac = pp[j];
+      for (int s = 1; s < nsplit; ++s) mac = mod_add(mac, pp[(size_t)s * P::N + j], q);
+      o[j] = mod_sub(mac, a[e], q);
+    }
   }
 }
 
@@ -621,6 +652,7 @@ static int setup_tail(Ctx &c, uint32_t *d_mpk, const uint32_t *d_msk, uint32_t *
     constexpr int LOGN = decltype(L)::value;
     constexpr int G = ppc<LOGN>();
     CUFE_CUDA(cudaFuncSetAttribute(k_setup_mpk<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    ProfScope ps("setup_mpk", s);
     k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
         d_msk, e, ahat, a_sh, d_mpk, nres, c.ring.args);
     CUFE_CUDA(cudaGetLastError());
@@ -683,6 +715,7 @@ static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *
     constexpr int LOGN = decltype(L)::value;
     constexpr int G = ppc<LOGN>();
     CUFE_CUDA(cudaFuncSetAttribute(k_encrypt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    ProfScope ps("encrypt_intt", s);
     k_encrypt<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
         d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
     CUFE_CUDA(cudaGetLastError());
@@ -763,6 +796,7 @@ int ctx_keygen(Ctx &c, int nkeys, const uint32_t *d_y, int y_signed, const uint3
   if (smem > 200 * 1024) return CUFE_ERR_INVALID;
   CUFE_CUDA(cudaFuncSetAttribute(k_keygen<KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((c.n + 255) / 256, 3, (nkeys + KCH - 1) / KCH);
+  ProfScope ps("keygen", s);
   k_keygen<KCH><<<grid, 256, smem, s>>>(d_y, y_signed, nkeys, d_msk, d_sky, c.n, sa);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
@@ -773,12 +807,19 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
   if (nct < 1 || nkeys < 1) return CUFE_ERR_INVALID;
   const int n = c.n, l = c.l;
   const size_t poly = (size_t)3 * n;
-  int rc = c.ensure_ws(((size_t)nct * poly + 2 * (size_t)nkeys * poly) * 4 + 4 * 256);
+  const long long nwork = (long long)nct * nkeys * 3;
+  // split the l-sum until about two waves of MAC threads are resident
+  const long long base_threads = nwork * (n / 4);
+  const long long want = (long long)c.num_sms * 2048 * 2;
+  int nsplit = 1;
+  while (nsplit < 32 && base_threads * nsplit < want && l / (nsplit * 2) >= 8) nsplit *= 2;
+  int rc = c.ensure_ws(((size_t)nct * poly + 2 * (size_t)nkeys * poly + (size_t)nwork * nsplit * n) * 4 + 8 * 256);
   if (rc) return rc;
   Arena ar(c.ws);
   uint32_t *clhat = ar.take<uint32_t>((size_t)nct * poly);
   uint32_t *skhat = ar.take<uint32_t>((size_t)nkeys * poly);
   uint32_t *skhat_sh = ar.take<uint32_t>((size_t)nkeys * poly);
+  uint32_t *part = ar.take<uint32_t>((size_t)nwork * nsplit * n);
   CUFE_CUDA(cudaMemcpy2DAsync(clhat, poly * 4, d_ct + (size_t)l * poly, (size_t)(l + 1) * poly * 4, poly * 4, nct,
                               cudaMemcpyDeviceToDevice, s));
   rc = ntt_launch(c.ring.args, clhat, (long long)nct * 3, false, s);
@@ -786,16 +827,26 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
   CUFE_CUDA(cudaMemcpyAsync(skhat, d_sky, (size_t)nkeys * poly * 4, cudaMemcpyDeviceToDevice, s));
   rc = ntt_fwd_shoup_launch(c.ring.args, skhat, skhat_sh, (long long)nkeys * 3, s);
   if (rc) return rc;
-  const long long nwork = (long long)nct * nkeys * 3;
   const SchemeArgs sa = scheme_args(c);
+  {
+    const int threads = std::min(256, n / 4);
+    const int per_poly = n / 4 / threads;
+    const size_t smem = (size_t)2 * ((l + nsplit - 1) / nsplit + 1) * 4;
+    if (smem > 200 * 1024) return CUFE_ERR_INVALID;
+    CUFE_CUDA(cudaFuncSetAttribute(k_dec_mac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ProfScope ps("decrypt_mac", s);
+    k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
+                                                                             part, sa);
+    CUFE_CUDA(cudaGetLastError());
+  }
   return dispatch_logn(c.ring.logn, [&](auto L) {
     constexpr int LOGN = decltype(L)::value;
     constexpr int G = ppc<LOGN>();
-    const size_t smem = (size_t)G * (NttPlan<LOGN>::N + 2 * l) * 4;
-    if (smem > 200 * 1024) return (int)CUFE_ERR_INVALID;
-    CUFE_CUDA(cudaFuncSetAttribute(k_decrypt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_decrypt<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
-        d_ct, clhat, skhat, skhat_sh, d_y, y_signed, nct, nkeys, d_dy, nwork, sa);
+    const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
+    CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    ProfScope ps("decrypt_tail", s);
+    k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
+        part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);
     CUFE_CUDA(cudaGetLastError());
     return (int)CUFE_OK;
   });
@@ -820,6 +871,7 @@ int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_
   d.p = c.p;
   d.n = c.n;
   const long long total = (long long)count * ncoeff;
+  ProfScope ps("decode", s);
   k_decode<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_dy, count, ncoeff, d_out, d);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;

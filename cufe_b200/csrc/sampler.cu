@@ -15,6 +15,7 @@
 #include "aes.cuh"
 #include "sampler.cuh"
 #include "sampler_host.h"
+#include "prof.h"
 
 #include <algorithm>
 
@@ -28,13 +29,23 @@ __device__ __forceinline__ uint64_t le64_of(uint32_t be_lo, uint32_t be_hi) {
 
 // ------------------------------------------------------------------ CPU mapping, phase 1
 
-template <int SIG>
-__device__ __noinline__ void uniform_slow(const uint32_t *U, uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
-                                          const AesCtx &c, uint32_t *status) {
+// one keystream block of the CPU mapping from round keys in global memory (rare paths)
+__device__ __noinline__ void ctr_block_g(uint32_t (&W)[4], uint32_t ctr, const uint32_t *__restrict__ rkg,
+                                         const AesCtx &c) {
   uint32_t rk[60];
 #pragma unroll
   for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
-  int w = 0;
+  aes256_ctr_block(W, 0u, ctr, rk, c);
+}
+
+// uniform draws when one of the first 8 words is rejected: rescan bytes 200.. with the
+// rejection loop of src/gauss.c:578-703, regenerating blocks as needed (about 7% of S2/S3
+// refills, practically never for S1)
+template <int SIG>
+__device__ __noinline__ void uniform_slow(uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
+                                          const AesCtx &c, uint32_t *status) {
+  int w = 0, have_blk = -1;
+  uint32_t W[4] = {0, 0, 0, 0};
   for (int j = 0; j < 8; ++j) {
     uint32_t x = 0;
     for (;;) {
@@ -43,14 +54,13 @@ __device__ __noinline__ void uniform_slow(const uint32_t *U, uint32_t *y, uint32
         x = 0;
         break;
       }
-      if (w < 22) {
-        x = U[w];
-      } else {
-        const int byte = 200 + 4 * w;
-        uint32_t W[4];
-        aes256_ctr_block(W, 0u, cb + (uint32_t)(byte >> 4), rk, c);
-        x = bswap32(W[(byte >> 2) & 3]);
+      const int byte = 200 + 4 * w, blk = byte >> 4;
+      if (blk != have_blk) {
+        ctr_block_g(W, cb + (uint32_t)blk, rkg, c);
+        have_blk = blk;
       }
+      const int wi = (byte >> 2) & 3;
+      x = bswap32(wi == 0 ? W[0] : wi == 1 ? W[1] : wi == 2 ? W[2] : W[3]);
       ++w;
       if (uniform_ok<SIG>(x)) break;
     }
@@ -58,11 +68,43 @@ __device__ __noinline__ void uniform_slow(const uint32_t *U, uint32_t *y, uint32
   }
 }
 
-// One refill of the CPU mapping: blocks needed for S1/S2 are 2-6 and 8-17 (bytes 32..287);
-// the 126-bit CDT of the CPU S3 additionally reads bytes 0..31 / 100..131, fetched only
-// when a high word ties a table entry.
+// 126-bit CDT compare of the CPU S3 for one lane whose high word ties a table entry: the
+// low word (bytes 8 lane.. of r, or of r + 100 for lanes 4..7) is regenerated here
+__device__ __noinline__ uint32_t cdt_full_slow(int lane, uint64_t r2, uint32_t cb, const uint32_t *__restrict__ rkg,
+                                               const AesCtx &c) {
+  const int off = (lane < 4 ? 0 : 100) + 8 * (lane & 3);
+  uint32_t W[4], lo, hi;
+  ctr_block_g(W, cb + (uint32_t)(off >> 4), rkg, c);
+  const int w0 = (off >> 2) & 3;
+  lo = w0 == 0 ? W[0] : w0 == 1 ? W[1] : w0 == 2 ? W[2] : W[3];
+  const int off2 = off + 4;
+  if ((off2 >> 4) != (off >> 4)) ctr_block_g(W, cb + (uint32_t)(off2 >> 4), rkg, c);
+  const int w1 = (off2 >> 2) & 3;
+  hi = w1 == 0 ? W[0] : w1 == 1 ? W[1] : w1 == 2 ? W[2] : W[3];
+  return cdt_sample<true>(r2, (uint64_t)bswap32(lo) | ((uint64_t)bswap32(hi) << 32));
+}
+
+template <bool FULL>
+__device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb, const uint32_t *rkg,
+                                             const AesCtx &c) {
+  if (FULL && cdt_needs_low(r2)) return cdt_full_slow(lane, r2, cb, rkg, c);
+  return cdt_sample<false>(r2, 0);
+}
+
+// Block consumption order of one refill (16-byte block b = bytes 16b..16b+15):
+//   12..17  uniform words (bytes 200..287, sign byte 280), kept: bytes 192..199
+//   2, 3    CDT high words of lanes 0..3 (bytes 32..63)
+//   6       exponent bytes of lanes 0..3 (96..99)
+//   4, 5    Bernoulli mantissas of lanes 0..3 (64..95)          -> lanes 0..3 done
+//   8..10   CDT high words of lanes 4..7 (132..163)
+//   10, 11  Bernoulli mantissas of lanes 4..7 (164..195)         -> lanes 4..7 done
+// Blocks 0, 1, 7 (and the low CDT words) are never needed by S1/S2 and only on ties by S3.
+__constant__ uint8_t c_block_order[15] = {12, 13, 14, 15, 16, 17, 2, 3, 6, 4, 5, 8, 9, 10, 11};
+
+constexpr int kCandThreads = 384;  // 1 CTA (128 KiB of tables) per SM; 168 registers per thread
+
 template <int SIG, bool FULL, int VAR>
-__global__ void __launch_bounds__(512, 1)
+__global__ void __launch_bounds__(kCandThreads, 1)
     k_cand_cpu(const uint32_t *__restrict__ rkeys, uint32_t nstreams, uint32_t refills, double kinv,
                int64_t *__restrict__ cand, uint8_t *__restrict__ amask, uint32_t *__restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -74,124 +116,134 @@ __global__ void __launch_bounds__(512, 1)
   uint32_t cur = 0xffffffffu;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const uint32_t st = g / refills, t = g - st * refills;
+    const uint32_t *rkg = rkeys + (size_t)st * 60;
     if (st != cur) {
 #pragma unroll
-      for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkeys + (size_t)st * 60 + i);
+      for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
       cur = st;
     }
     const uint32_t cb = t * 24u;
-    uint32_t W[4];
-    // ---- uniform words (bytes 200..287) and the sign byte 280
-    uint32_t U[22], keep0, keep1;
-    aes256_ctr_block(W, 0u, cb + 12u, rk, c);
-    keep0 = W[0];
-    keep1 = W[1];
-    U[0] = bswap32(W[2]);
-    U[1] = bswap32(W[3]);
-#pragma unroll
-    for (int b = 13; b < 18; ++b) {
-      aes256_ctr_block(W, 0u, cb + (uint32_t)b, rk, c);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) U[2 + 4 * (b - 13) + i] = bswap32(W[i]);
-    }
-    const uint32_t k8 = U[20] & 0xffu;
-    uint32_t y[8];
-    bool fast = true;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) fast &= uniform_ok<SIG>(U[i]);
-    if (fast) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) y[i] = uniform_reduce<SIG>(U[i]);
-    } else {
-      uint32_t Ul[22], yl[8];
-#pragma unroll
-      for (int i = 0; i < 22; ++i) Ul[i] = U[i];
-      uniform_slow<SIG>(Ul, yl, cb, rkeys + (size_t)st * 60, c, status);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) y[i] = yl[i];
-    }
-    uint64_t z[8];
-    uint32_t acc = 0;
-    // ---- lanes 0..3: CDT high words at 32..63, Bernoulli bytes 64..99
-    {
-      uint32_t A[4], B[4];
-      aes256_ctr_block(A, 0u, cb + 2u, rk, c);
-      aes256_ctr_block(B, 0u, cb + 3u, rk, c);
-      const uint64_t r2[4] = {le64_of(A[0], A[1]), le64_of(A[2], A[3]), le64_of(B[0], B[1]),
-                              le64_of(B[2], B[3])};
-      uint32_t x[4];
-      bool low = false;
-      if (FULL) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) low |= cdt_needs_low(r2[i]);
-      }
-      if (FULL && low) {
-        aes256_ctr_block(A, 0u, cb + 0u, rk, c);
-        aes256_ctr_block(B, 0u, cb + 1u, rk, c);
-        const uint64_t r1[4] = {le64_of(A[0], A[1]), le64_of(A[2], A[3]), le64_of(B[0], B[1]),
-                                le64_of(B[2], B[3])};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<FULL>(r2[i], r1[i]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<false>(r2[i], 0);
-      }
-      uint32_t M4[4], M5[4], M6[4];
-      aes256_ctr_block(M4, 0u, cb + 4u, rk, c);
-      aes256_ctr_block(M5, 0u, cb + 5u, rk, c);
-      aes256_ctr_block(M6, 0u, cb + 6u, rk, c);
-      const uint64_t rm[4] = {le64_of(M4[0], M4[1]), le64_of(M4[2], M4[3]), le64_of(M5[0], M5[1]),
-                              le64_of(M5[2], M5[3])};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const uint32_t rexp = (M6[0] >> (24 - 8 * i)) & 0xffu;
-        const bool b = candidate<SIG, VAR>(x[i], y[i], rm[i], rexp, kinv, z[i]);
-        const uint32_t k = (k8 >> i) & 1u;
-        acc |= (uint32_t)accept_final(b, z[i], k) << i;
-      }
-      // ---- lanes 4..7: CDT high words at 132..163, Bernoulli bytes 164..199
-      uint32_t B8[4], B9[4], B10[4], B11[4];
-      aes256_ctr_block(B8, 0u, cb + 8u, rk, c);
-      aes256_ctr_block(B9, 0u, cb + 9u, rk, c);
-      aes256_ctr_block(B10, 0u, cb + 10u, rk, c);
-      const uint64_t s2[4] = {le64_of(B8[1], B8[2]), le64_of(B8[3], B9[0]), le64_of(B9[1], B9[2]),
-                              le64_of(B9[3], B10[0])};
-      bool low2 = false;
-      if (FULL) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) low2 |= cdt_needs_low(s2[i]);
-      }
-      if (FULL && low2) {
-        uint32_t B7[4];
-        aes256_ctr_block(B7, 0u, cb + 7u, rk, c);
-        const uint64_t s1[4] = {le64_of(M6[1], M6[2]), le64_of(M6[3], B7[0]), le64_of(B7[1], B7[2]),
-                                le64_of(B7[3], B8[0])};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<FULL>(s2[i], s1[i]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = cdt_sample<false>(s2[i], 0);
-      }
-      aes256_ctr_block(B11, 0u, cb + 11u, rk, c);
-      const uint64_t sm[4] = {le64_of(B10[1], B10[2]), le64_of(B10[3], B11[0]), le64_of(B11[1], B11[2]),
-                              le64_of(B11[3], keep0)};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const uint32_t rexp = (keep1 >> (24 - 8 * i)) & 0xffu;
-        const bool b = candidate<SIG, VAR>(x[i], y[4 + i], sm[i], rexp, kinv, z[4 + i]);
-        const uint32_t k = (k8 >> (4 + i)) & 1u;
-        acc |= (uint32_t)accept_final(b, z[4 + i], k) << (4 + i);
-      }
-    }
-    int64_t v[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t zi = (int64_t)z[i];
-      v[i] = ((k8 >> i) & 1u) ? -zi : zi;
-    }
     longlong2 *dst = reinterpret_cast<longlong2 *>(cand + (size_t)g * 8);
+    uint32_t U[22];
+    uint32_t keep0 = 0, keep1 = 0, k8 = 0, e6 = 0, carry = 0, acc = 0;
+    uint32_t y[8];
+    uint32_t x01 = 0, x23 = 0, x45 = 0, x67 = 0;  // CDT samples, two lanes per word
+#pragma unroll 1
+    for (int bi = 0; bi < 15; ++bi) {
+      uint32_t W[4];
+      aes256_ctr_block(W, 0u, cb + c_block_order[bi], rk, c);
+      // the pair of lanes completed by this block, if any
+      int lane0 = -1;
+      uint32_t xa = 0, xb = 0, ya = 0, yb = 0, ea = 0, eb = 0;
+      uint64_t ma = 0, mb = 0;
+      switch (bi) {
+        case 0:
+          keep0 = W[0];
+          keep1 = W[1];
+          U[0] = bswap32(W[2]);
+          U[1] = bswap32(W[3]);
+          break;
+        case 1: U[2] = bswap32(W[0]); U[3] = bswap32(W[1]); U[4] = bswap32(W[2]); U[5] = bswap32(W[3]); break;
+        case 2: U[6] = bswap32(W[0]); U[7] = bswap32(W[1]); U[8] = bswap32(W[2]); U[9] = bswap32(W[3]); break;
+        case 3: U[10] = bswap32(W[0]); U[11] = bswap32(W[1]); U[12] = bswap32(W[2]); U[13] = bswap32(W[3]); break;
+        case 4: U[14] = bswap32(W[0]); U[15] = bswap32(W[1]); U[16] = bswap32(W[2]); U[17] = bswap32(W[3]); break;
+        case 5: {
+          U[18] = bswap32(W[0]);
+          U[19] = bswap32(W[1]);
+          U[20] = bswap32(W[2]);
+          U[21] = bswap32(W[3]);
+          k8 = U[20] & 0xffu;
+          bool fast = true;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) dst[i] = make_longlong2(v[2 * i], v[2 * i + 1]);
+          for (int i = 0; i < 8; ++i) fast &= uniform_ok<SIG>(U[i]);
+          if (fast) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) y[i] = uniform_reduce<SIG>(U[i]);
+          } else {
+            uint32_t yl[8];
+            uniform_slow<SIG>(yl, cb, rkg, c, status);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) y[i] = yl[i];
+          }
+          break;
+        }
+        case 6:  // block 2: lanes 0, 1
+          x01 = cdt_lane<FULL>(0, le64_of(W[0], W[1]), cb, rkg, c) |
+                (cdt_lane<FULL>(1, le64_of(W[2], W[3]), cb, rkg, c) << 16);
+          break;
+        case 7:  // block 3: lanes 2, 3
+          x23 = cdt_lane<FULL>(2, le64_of(W[0], W[1]), cb, rkg, c) |
+                (cdt_lane<FULL>(3, le64_of(W[2], W[3]), cb, rkg, c) << 16);
+          break;
+        case 8:  // block 6: exponent bytes of lanes 0..3
+          e6 = W[0];
+          break;
+        case 9:  // block 4: lanes 0, 1
+          lane0 = 0;
+          xa = x01 & 0xffffu; xb = x01 >> 16; ya = y[0]; yb = y[1];
+          ma = le64_of(W[0], W[1]); mb = le64_of(W[2], W[3]);
+          ea = e6 >> 24; eb = (e6 >> 16) & 0xffu;
+          break;
+        case 10:  // block 5: lanes 2, 3
+          lane0 = 2;
+          xa = x23 & 0xffffu; xb = x23 >> 16; ya = y[2]; yb = y[3];
+          ma = le64_of(W[0], W[1]); mb = le64_of(W[2], W[3]);
+          ea = (e6 >> 8) & 0xffu; eb = e6 & 0xffu;
+          break;
+        case 11:  // block 8: lane 4 (132..139), first half of lane 5
+          x45 = cdt_lane<FULL>(4, le64_of(W[1], W[2]), cb, rkg, c);
+          carry = W[3];
+          break;
+        case 12:  // block 9: rest of lane 5, lane 6, first half of lane 7
+          x45 |= cdt_lane<FULL>(5, le64_of(carry, W[0]), cb, rkg, c) << 16;
+          x67 = cdt_lane<FULL>(6, le64_of(W[1], W[2]), cb, rkg, c);
+          carry = W[3];
+          break;
+        case 13:  // block 10: rest of lane 7 (CDT); mantissa of lane 4, half of lane 5
+          x67 |= cdt_lane<FULL>(7, le64_of(carry, W[0]), cb, rkg, c) << 16;
+          lane0 = 4;
+          xa = x45 & 0xffffu; ya = y[4];
+          ma = le64_of(W[1], W[2]);
+          ea = keep1 >> 24;
+          carry = W[3];
+          break;
+        case 14:  // block 11: rest of lane 5's mantissa, lanes 6 and 7 (7 ends in bytes 192..195)
+          lane0 = 5;
+          break;
+      }
+      if (bi == 14) {
+        // lanes 5, 6, 7 complete here
+        const uint64_t m5 = le64_of(carry, W[0]), m6 = le64_of(W[1], W[2]), m7 = le64_of(W[3], keep0);
+        uint64_t z5, z6, z7;
+        const bool b5 = candidate<SIG, VAR>(x45 >> 16, y[5], m5, (keep1 >> 16) & 0xffu, kinv, z5);
+        const bool b6 = candidate<SIG, VAR>(x67 & 0xffffu, y[6], m6, (keep1 >> 8) & 0xffu, kinv, z6);
+        const bool b7 = candidate<SIG, VAR>(x67 >> 16, y[7], m7, keep1 & 0xffu, kinv, z7);
+        acc |= (uint32_t)accept_final(b5, z5, (k8 >> 5) & 1u) << 5;
+        acc |= (uint32_t)accept_final(b6, z6, (k8 >> 6) & 1u) << 6;
+        acc |= (uint32_t)accept_final(b7, z7, (k8 >> 7) & 1u) << 7;
+        const int64_t v5 = ((k8 >> 5) & 1u) ? -(int64_t)z5 : (int64_t)z5;
+        const int64_t v6 = ((k8 >> 6) & 1u) ? -(int64_t)z6 : (int64_t)z6;
+        const int64_t v7 = ((k8 >> 7) & 1u) ? -(int64_t)z7 : (int64_t)z7;
+        // lane 4 was stored as the first half of pair (4, 5) in block 10
+        reinterpret_cast<int64_t *>(dst)[5] = v5;
+        dst[3] = make_longlong2(v6, v7);
+      } else if (lane0 >= 0) {
+        uint64_t za, zb = 0;
+        const bool ba = candidate<SIG, VAR>(xa, ya, ma, ea, kinv, za);
+        const uint32_t ka = (k8 >> lane0) & 1u;
+        acc |= (uint32_t)accept_final(ba, za, ka) << lane0;
+        const int64_t va = ka ? -(int64_t)za : (int64_t)za;
+        if (lane0 == 4) {
+          reinterpret_cast<int64_t *>(dst)[4] = va;
+        } else {
+          const bool bb = candidate<SIG, VAR>(xb, yb, mb, eb, kinv, zb);
+          const uint32_t kb = (k8 >> (lane0 + 1)) & 1u;
+          acc |= (uint32_t)accept_final(bb, zb, kb) << (lane0 + 1);
+          const int64_t vb = kb ? -(int64_t)zb : (int64_t)zb;
+          dst[lane0 >> 1] = make_longlong2(va, vb);
+        }
+      }
+    }
     amask[g] = (uint8_t)acc;
   }
 }
@@ -656,19 +708,26 @@ int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t
   uint32_t *cstart = reinterpret_cast<uint32_t *>(take((size_t)nstreams * (calls + 1) * 4));
   const double kinv = kinv_of(sig);
   const uint32_t total = nstreams * R;
-  const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (total + 511) / 512);
+  const uint32_t grid =
+      (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (total + kCandThreads - 1) / kCandThreads);
+  {
+  ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
   if (sig == 0)
-    k_cand_cpu<0, false, 0><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+    k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
   else if (sig == 1)
-    k_cand_cpu<1, false, 0><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+    k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
   else
-    k_cand_cpu<2, true, 1><<<grid, 512, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+    k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+  }
   CUFE_CUDA(cudaGetLastError());
+  { ProfScope ps("sample_scan", s);
   k_scan_tiles<<<dim3(tiles, nstreams), 512, 0, s>>>(amask, R, tiles, elocal, tsum);
-  k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles);
+  k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles); }
   const uint32_t guess = (uint32_t)((double)n / mean_accept(sig));
+  { ProfScope ps("sample_walk", s);
   k_walk<<<(nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, R, tiles, calls, n, guess, nstreams, cstart,
-                                            d_status);
+                                            d_status); }
+  ProfScope ps_sc("sample_scatter", s);
   k_scatter<<<dim3(calls, nstreams), 256, 0, s>>>(cand, amask, elocal, tsum, cstart, R, tiles, calls, n, mod_args(),
                                                   d_out);
   CUFE_CUDA(cudaGetLastError());
@@ -680,6 +739,7 @@ int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npo
   const uint32_t threads = npolys * (n / 8);
   const uint32_t grid = (threads + 255) / 256;
   const double kinv = kinv_of(sig);
+  ProfScope ps("sample_gpu_map", s);
   if (sig == 0)
     k_gauss_gpu_map<0><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
   else if (sig == 1)
@@ -692,6 +752,7 @@ int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npo
 
 int sample_polya(const uint32_t *d_rkey, uint32_t n, uint32_t *d_a, cudaStream_t s) {
   const uint32_t grid = (n / 2 + 255) / 256;
+  ProfScope ps("sample_polya", s);
   k_polya<<<grid, 256, kAesSmemBytes, s>>>(d_rkey, n, mod_args(), d_a);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;

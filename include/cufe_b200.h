@@ -84,6 +84,13 @@ int cufe_destroy(cufe_ctx *ctx);
 int cufe_sync(cufe_ctx *ctx, void *stream);
 /* a non-blocking stream owned by the context */
 void *cufe_ctx_stream(cufe_ctx *ctx);
+/* per-kernel device timing: when enabled, every kernel this context launches is bracketed
+ * by CUDA events on its stream; cufe_profile_read waits for them and returns, per kernel
+ * name (64-byte slots), the launch count and the summed milliseconds; returns the number
+ * of kernels written (or a negative status) */
+int cufe_profile_enable(cufe_ctx *ctx, int on);
+int cufe_profile_read(cufe_ctx *ctx, int max_kernels, char *names, long long *launches, double *ms);
+int cufe_profile_reset(cufe_ctx *ctx);
 /* p and floor(q/p) mod q_j */
 int cufe_params(const cufe_ctx *ctx, uint32_t *p, uint32_t delta_mod[3]);
 /* twiddle tables [3][n] (psi^{bitrev(i)}, psi^{-bitrev(i)}) in host memory */
@@ -124,6 +131,9 @@ int cufe_decode(cufe_ctx *ctx, int count, const uint32_t *d_dy, int ncoeff, uint
  * gaussian_sampler_S* calls of n samples (src/gauss.c:789,995,1086): d_out[nstreams][calls][3][n]. */
 int cufe_sample_cpu_map(cufe_ctx *ctx, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
                         void *stream);
+/* refills (384-byte AES-CTR blocks of 8 candidates) that the CPU-mapping sampler
+ * precomputes per stream for `calls` calls of n samples (sizing and roofline accounting) */
+long long cufe_sampler_refills(int sig, int calls, int n);
 /* GPU counter mapping (src/sample_gpu.cu:40-289) for polynomials poly0..poly0+npolys-1 */
 int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0, int npolys, uint32_t *d_out,
                         void *stream);
