@@ -60,6 +60,7 @@ def lib():
             "cufe_encrypt_gpu_map": [vp, i, vp, vp, vp, vp, vp],
             "cufe_keygen": [vp, i, vp, i, vp, vp, vp],
             "cufe_decrypt": [vp, i, vp, i, vp, i, vp, vp, vp],
+            "cufe_decrypt_noalloc": [vp, vp, i, vp, i, vp, vp, vp],
             "cufe_decode": [vp, i, vp, i, vp, vp],
             "cufe_sample_cpu_map": [vp, i, i, vp, i, vp, vp],
             "cufe_sample_gpu_map": [vp, i, vp, i, i, vp, vp],
@@ -247,6 +248,14 @@ class Context:
         dy = _dev((nct, nkeys, 3, self.n), self.dev) if dy is None else dy
         _check(lib().cufe_decrypt(self.h, nct, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(dy), _stream(stream, self.device)),
                "cufe_decrypt")
+        return dy
+
+    def decrypt_noalloc(self, ct, y, sky, y_signed=False, dy=None, stream=None):
+        """decryption of one ciphertext with up to 4 keys, no device allocation in the call"""
+        nkeys = y.shape[0]
+        dy = _dev((1, nkeys, 3, self.n), self.dev) if dy is None else dy
+        _check(lib().cufe_decrypt_noalloc(self.h, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(dy),
+                                          _stream(stream, self.device)), "cufe_decrypt_noalloc")
         return dy
 
     def decode(self, dy, ncoeff=None, out=None, stream=None):

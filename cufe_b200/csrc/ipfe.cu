@@ -7,6 +7,8 @@
 // d_y = sum y_i c_i - c_l * sk_y, decoded as round(p d_y / q).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "ctx.h"
 #include "ntt.cuh"
@@ -845,6 +847,100 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
     const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     ProfScope ps("decrypt_tail", s);
+    k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
+        part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);
+    CUFE_CUDA(cudaGetLastError());
+    return (int)CUFE_OK;
+  });
+}
+
+// ------------------------------------------------------------------ decryption without allocation
+//
+// Some callers cannot call cudaMalloc while they decrypt: a host application that hands this
+// library a fixed GPU memory budget up front, or a latency-critical serving thread that must
+// not take the implicit device synchronisation of a cudaMalloc/cudaFree.  For them,
+// ctx_decrypt_noalloc runs the same decryption kernels as ctx_decrypt with every scratch
+// buffer carved from the file-scope array below instead of the context workspace.  The
+// array is a fixed part of the library image: every GPU that loads the library holds its
+// 2 MiB until the process exits.
+constexpr int kNoAllocMaxN = 4096;    // ring degree
+constexpr int kNoAllocMaxKeys = 4;    // keys per call (one ciphertext per call)
+constexpr int kNoAllocMaxSplit = 8;   // chunks of the l-sum
+constexpr size_t kNoAllocWords = (size_t)3 * kNoAllocMaxN                       // NTT(c_l)
+                                 + (size_t)2 * kNoAllocMaxKeys * 3 * kNoAllocMaxN  // NTT(sk_y), Shoup
+                                 + (size_t)3 * kNoAllocMaxKeys * kNoAllocMaxSplit * kNoAllocMaxN  // partials
+                                 + 4 * 64;                                          // region padding
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+// Host code may not use g_noalloc_scratch as an address: it is only a host-side stand-in for
+// the symbol.  The device address comes from cudaGetSymbolAddress, once per device, with that
+// device current (the first call on a device does it; make that first call before any stream
+// capture).
+static std::mutex g_noalloc_mu;
+static uint32_t *g_noalloc_dev[64] = {};
+
+static int noalloc_scratch(int device, uint32_t **out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= 64) return CUFE_ERR_INVALID;
+  if (!g_noalloc_dev[device]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_last_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      return CUFE_ERR_CUDA;
+    }
+    g_noalloc_dev[device] = static_cast<uint32_t *>(ptr);
+  }
+  *out = g_noalloc_dev[device];
+  return CUFE_OK;
+}
+
+int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                        const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s) {
+  const int n = c.n, l = c.l;
+  if (n > kNoAllocMaxN || nkeys < 1 || nkeys > kNoAllocMaxKeys) {
+    set_last_error("cufe_decrypt_noalloc supports n <= " + std::to_string(kNoAllocMaxN) + " and 1.." +
+                   std::to_string(kNoAllocMaxKeys) + " keys per call (got n = " + std::to_string(n) +
+                   ", keys = " + std::to_string(nkeys) + ")");
+    return CUFE_ERR_INVALID;
+  }
+  uint32_t *base = nullptr;
+  int rc = noalloc_scratch(c.device, &base);
+  if (rc) return rc;
+  const size_t poly = (size_t)3 * n;
+  const long long nwork = (long long)nkeys * 3;
+  const long long base_threads = nwork * (n / 4);
+  const long long want = (long long)c.num_sms * 2048 * 2;
+  int nsplit = 1;
+  while (nsplit < kNoAllocMaxSplit && base_threads * nsplit < want && l / (nsplit * 2) >= 8) nsplit *= 2;
+  auto round64 = [](size_t w) { return (w + 63) & ~(size_t)63; };
+  uint32_t *clhat = base;
+  uint32_t *skhat = clhat + round64(poly);
+  uint32_t *skhat_sh = skhat + round64((size_t)nkeys * poly);
+  uint32_t *part = skhat_sh + round64((size_t)nkeys * poly);
+  // every scratch word read below is written first by this call (no zeroing needed)
+  CUFE_CUDA(cudaMemcpyAsync(clhat, d_ct + (size_t)l * poly, poly * 4, cudaMemcpyDeviceToDevice, s));
+  rc = ntt_launch(c.ring.args, clhat, 3, false, s);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMemcpyAsync(skhat, d_sky, (size_t)nkeys * poly * 4, cudaMemcpyDeviceToDevice, s));
+  rc = ntt_fwd_shoup_launch(c.ring.args, skhat, skhat_sh, (long long)nkeys * 3, s);
+  if (rc) return rc;
+  const SchemeArgs sa = scheme_args(c);
+  {
+    const int threads = std::min(256, n / 4);
+    const int per_poly = n / 4 / threads;
+    const size_t smem = (size_t)2 * ((l + nsplit - 1) / nsplit + 1) * 4;
+    if (smem > 200 * 1024) return CUFE_ERR_INVALID;
+    CUFE_CUDA(cudaFuncSetAttribute(k_dec_mac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
+                                                                             part, sa);
+    CUFE_CUDA(cudaGetLastError());
+  }
+  return dispatch_logn(c.ring.logn, [&](auto L) {
+    constexpr int LOGN = decltype(L)::value;
+    constexpr int G = ppc<LOGN>();
+    const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
+    CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
         part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);
     CUFE_CUDA(cudaGetLastError());

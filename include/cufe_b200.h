@@ -122,6 +122,18 @@ int cufe_keygen(cufe_ctx *ctx, int nkeys, const uint32_t *d_y, int y_signed, con
  * src/rlwe_sife.c:248-278) for every (ciphertext, key) pair: d_dy[nct][nkeys][3][n] */
 int cufe_decrypt(cufe_ctx *ctx, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                  const uint32_t *d_sky, uint32_t *d_dy, void *stream);
+/* Decryption that allocates no device memory, for callers that cannot call cudaMalloc
+ * during a call (a host application with a fixed GPU memory budget, or a serving thread
+ * that must not take cudaMalloc's implicit device synchronisation).  No counterpart in the
+ * reference.  Same result as cufe_decrypt for one ciphertext d_ct[l+1][3][n] and nkeys
+ * keys: d_dy[nkeys][3][n].  Limits: n <= 4096 and 1 <= nkeys <= 4, else CUFE_ERR_INVALID.
+ * Its scratch is a fixed array of about 2 MiB inside the library image, held on every GPU
+ * that loads the library until the process exits.  The first call on a device looks up the
+ * array's device address (make that first call before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU (different streams, threads or contexts without
+ * ordering between them) race and corrupt each other's results. */
+int cufe_decrypt_noalloc(cufe_ctx *ctx, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                         const uint32_t *d_sky, uint32_t *d_dy, void *stream);
 /* crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332) on the first
  * ncoeff coefficients of each of count d_y: d_out[count][ncoeff], values in [0, p] */
 int cufe_decode(cufe_ctx *ctx, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, void *stream);
