@@ -45,6 +45,17 @@ def workload():
     return x, y, seeds2, seeds3, setup_seeds
 
 
+def max_over_ranks(value, device):
+    """max of a per-rank float over the process group (identity without one)"""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -258,10 +269,7 @@ def gpu_arm(args):
     prof = ctx.profile_read()
     ctx.sync()
     step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(steps)]
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dev)
     # correctness of every inner product in the timed region
     got = cf.u32(res[:, :, 0]).astype(np.int64)
     p = ctx.p
@@ -308,10 +316,7 @@ def gpu_arm(args):
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_ok = bool((np.where(rh.numpy().view(np.uint32).astype(np.int64) > p // 2,
                             rh.numpy().view(np.uint32).astype(np.int64) - p,
                             rh.numpy().view(np.uint32).astype(np.int64)) == exp).all())

@@ -46,9 +46,15 @@ static int need_device(int device) {
   return CUFE_OK;
 }
 
+static bool pow2_in(int n, int lo, int hi) { return n >= lo && n <= hi && (n & (n - 1)) == 0; }
+
 int cufe_create(cufe_ctx **out, int n, int l, int device) {
   if (!out) return CUFE_ERR_INVALID;
   *out = nullptr;
+  if (!pow2_in(n, 16, 8192) || l < 1 || l > 65536) {
+    cufe::set_last_error("n must be a power of two in [16, 8192] and l in [1, 65536]");
+    return CUFE_ERR_INVALID;
+  }
   int rc = need_device(device);
   if (rc) return rc;
   cufe_ctx *h = new (std::nothrow) cufe_ctx();
@@ -214,6 +220,16 @@ int cufe_sample_polya(cufe_ctx *h, const uint8_t seed[32], uint32_t *d_a, void *
 int cufe_ring_create(cufe_ring **out, int n, int k, const uint32_t *primes, int device) {
   if (!out) return CUFE_ERR_INVALID;
   *out = nullptr;
+  if (!pow2_in(n, 16, 8192) || k < 1 || k > cufe::kMaxModuli) {
+    cufe::set_last_error("n must be a power of two in [16, 8192] and k in [1, 6]");
+    return CUFE_ERR_INVALID;
+  }
+  if (primes)
+    for (int m = 0; m < k; ++m)
+      if (primes[m] >= (1u << 31) || (primes[m] - 1) % (2u * (uint32_t)n) != 0) {
+        cufe::set_last_error("primes must be below 2^31 and 1 mod 2n");
+        return CUFE_ERR_INVALID;
+      }
   int rc = need_device(device);
   if (rc) return rc;
   cufe_ring *h = new (std::nothrow) cufe_ring();

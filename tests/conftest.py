@@ -11,6 +11,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+    config.addinivalue_line("markers", "slow: CPU test taking more than a few seconds")
 
 
 @pytest.fixture(scope="session")

@@ -1,0 +1,139 @@
+"""The oracle (oracle/cufe_oracle.c) against the reference's own CPU build: committed golden
+fixtures (tests/golden/, made by make_golden.py from oracle/_ref) and, where the compiled
+reference is present, fresh random cases.  CPU only."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.ffi import Oracle, Q, aes256_block, aes256_expand, canon, ctr_stream
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def gold(oracle_built):
+    d = np.load(os.path.join(GOLD, "ref_n256_l8.npz"))
+    return {k: d[k] for k in d.files}
+
+
+def test_aes256_fips197_kat(oracle_built):
+    # FIPS-197 appendix C.3
+    key = np.arange(32, dtype=np.uint8)
+    pt = np.frombuffer(bytes.fromhex("00112233445566778899aabbccddeeff"), np.uint8)
+    ct = aes256_block(aes256_expand(key), pt)
+    assert bytes(ct).hex() == "8ea2b7ca516745bfeafc49904b496089"
+
+
+def test_aes256_random_keys_match_cryptography(oracle_built):
+    mod = pytest.importorskip("cryptography.hazmat.primitives.ciphers")
+    rng = np.random.default_rng(1)
+    for _ in range(20):
+        key = rng.integers(0, 256, 32, dtype=np.uint8)
+        pt = rng.integers(0, 256, 16, dtype=np.uint8)
+        enc = mod.Cipher(mod.algorithms.AES(bytes(key)), mod.modes.ECB()).encryptor()
+        assert bytes(aes256_block(aes256_expand(key), pt)) == enc.update(bytes(pt)) + enc.finalize()
+
+
+def test_ctr_streams(gold):
+    assert (ctr_stream(gold["ctr_key"], 2) == gold["ctr_keyed"]).all()
+    assert (ctr_stream(None, 2) == gold["ctr_zero"]).all()
+
+
+def test_ntt_vectors(gold):
+    O = Oracle(256, 8)
+    for sel in range(3):
+        a = gold["ntt_in_%d" % sel]
+        assert (O.ntt(a, sel) == gold["ntt_fwd_%d" % sel]).all()
+        assert (O.ntt(a, sel, inverse=True) == gold["ntt_inv_%d" % sel]).all()
+
+
+@pytest.mark.parametrize("sig", [0, 1, 2])
+def test_sampler_streams(gold, sig):
+    O = Oracle(256, 8)
+    got, _ = O.gauss(sig, gold["ctr_key"], 4)
+    assert (canon(got) == gold["gauss_key_%d" % sig]).all()
+    got, _ = O.gauss(sig, None, 4)
+    assert (canon(got) == gold["gauss_zero_%d" % sig]).all()
+
+
+def test_scheme_round_trip(gold):
+    O = Oracle(256, 8)
+    assert (O.sample_polya(gold["polya_seed"]) == gold["polya"]).all()
+    mpk, msk = O.setup(gold["seed_a"], None, gold["seed_e"])
+    assert (canon(mpk) == gold["mpk"]).all() and (canon(msk) == gold["msk"]).all()
+    ct = O.encrypt(gold["x"], mpk, gold["seed2"], None)
+    assert (canon(ct) == gold["ct"]).all()
+    sky = O.keygen(gold["y"], msk)
+    assert (canon(sky) == gold["sky"]).all()
+    dy = O.decrypt(ct, gold["y"], sky)
+    assert (canon(dy) == gold["dy"]).all()
+    dec = O.decode(dy)
+    assert (dec == gold["dec"]).all()
+    assert int(dec[0]) == int(gold["x"].astype(np.int64) @ gold["y"].astype(np.int64))
+
+
+@pytest.mark.slow
+def test_c2_shape_hashes(oracle_built):
+    doc = json.load(open(os.path.join(GOLD, "ref_c2.json")))
+    n, l = doc["n"], doc["l"]
+    rng = np.random.default_rng(0xC0FE0002)
+    seed_a, seed_e, seed2 = rng.integers(0, 256, (3, 32), dtype=np.uint8)
+    x = rng.integers(0, 5, l, dtype=np.uint32)
+    y = rng.integers(0, 17, l, dtype=np.uint32)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    O = Oracle(n, l)
+    mpk, msk = O.setup(seed_a, None, seed_e)
+    assert sha(canon(mpk)) == doc["mpk"] and sha(canon(msk)) == doc["msk"]
+    ct = O.encrypt(x, mpk, seed2, None)
+    assert sha(canon(ct)) == doc["ct"]
+    sky = O.keygen(y, msk)
+    dy = O.decrypt(ct, y, sky)
+    assert sha(canon(sky)) == doc["sky"] and sha(canon(dy)) == doc["dy"]
+    dec = O.decode(dy)
+    assert sha(dec) == doc["dec"] and int(dec[0]) == doc["ip"] == doc["ip_plain"]
+
+
+def test_parameters(oracle_built):
+    for n in (16, 256, 2048, 4096):
+        t = Oracle(n, 8).tables()
+        t4 = Oracle(4096, 8).tables()
+        assert (t["psi"] == t4["psi"][:, :n]).all()  # one chain of tables for every n
+        for j, q in enumerate(Q):
+            assert pow(int(t["psi"][j][n // 2]), n, q) == q - 1  # primitive 2n-th root
+            assert int(t["ninv"][j]) * n % q == 1
+    t = Oracle(256, 785).tables()
+    assert t["p"] == 50241 and t["q"] == 76687145727357674227351553
+    assert t["delta"] == 1526385735302993058007  # src/params.h:27-28 values for l = 785
+    assert list(t["delta_mod"]) == [13798054, 441557681, 1912932552]
+
+
+def _have_ref(variant):
+    return os.path.exists(os.path.join(os.path.dirname(GOLD), "..", "oracle", "_ref", variant, "libref.so"))
+
+
+@pytest.mark.skipif(not _have_ref("n1024_l16"), reason="reference CPU build not present")
+def test_random_cases_against_reference_build(oracle_built):
+    from oracle.ffi import Reference
+    R = Reference("n1024_l16")
+    O = Oracle(1024, 16)
+    rng = np.random.default_rng(99)
+    for trial in range(3):
+        sa, se, s2 = rng.integers(0, 256, (3, 32), dtype=np.uint8)
+        mpk, msk = R.setup(sa, se)
+        omp, oms = O.setup(sa, None, se)
+        assert (mpk == omp).all() and (msk == oms).all()
+        x = rng.integers(0, 5, 16, dtype=np.uint32)
+        y = rng.integers(0, 17, 16, dtype=np.uint32)
+        ct = R.encrypt(x, mpk, s2)
+        assert (ct == O.encrypt(x, omp, s2, None)).all()
+        sk = R.keygen(y, msk)
+        assert (sk == O.keygen(y, oms)).all()
+        dy, dec = R.decrypt(ct, y, sk)
+        ody = O.decrypt(ct, y, sk)
+        assert (dy == canon(ody)).all() and (dec == O.decode(ody)).all()
+    for sig in range(3):
+        key = rng.integers(0, 256, 32, dtype=np.uint8)
+        assert (R.gauss(sig, key, 20) == O.gauss(sig, key, 20)[0]).all()
