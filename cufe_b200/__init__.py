@@ -29,10 +29,10 @@ class CufeError(RuntimeError):
         super().__init__("%s: %s (%d) %s" % (what, ERRORS.get(code, "error"), code, msg))
 
 
-def build(force=False):
-    """Compile the CUDA sources into the in-tree shared library."""
-    from . import build as _b
-    return _b.build(force=force)
+def compile_library(force=False):
+    """Compile the CUDA sources into the in-tree shared library (cufe_b200/build.py)."""
+    import importlib
+    return importlib.import_module("cufe_b200.build").build(force=force)
 
 
 def lib():
