@@ -38,9 +38,9 @@ __device__ __noinline__ void ctr_block_g(uint32_t (&W)[4], uint32_t ctr, const u
   aes256_ctr_block(W, 0u, ctr, rk, c);
 }
 
-// uniform draws when one of the first 8 words is rejected: rescan bytes 200.. with the
-// rejection loop of src/gauss.c:578-703, regenerating blocks as needed (about 7% of S2/S3
-// refills, practically never for S1)
+// uniform draws when the first 12 words hold fewer than 8 accepted ones (probability below
+// 1e-7 per refill): rescan bytes 200.. with the rejection loop of src/gauss.c:578-703,
+// regenerating blocks as needed
 template <int SIG>
 __device__ __noinline__ void uniform_slow(uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
                                           const AesCtx &c, uint32_t *status) {
@@ -91,17 +91,18 @@ __device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb,
   return cdt_sample<false>(r2, 0);
 }
 
-// Block consumption order of one refill (16-byte block b = bytes 16b..16b+15):
-//   12..17  uniform words (bytes 200..287, sign byte 280), kept: bytes 192..199
-//   2, 3    CDT high words of lanes 0..3 (bytes 32..63)
-//   6       exponent bytes of lanes 0..3 (96..99)
-//   4, 5    Bernoulli mantissas of lanes 0..3 (64..95)          -> lanes 0..3 done
-//   8..10   CDT high words of lanes 4..7 (132..163)
-//   10, 11  Bernoulli mantissas of lanes 4..7 (164..195)         -> lanes 4..7 done
-// Blocks 0, 1, 7 (and the low CDT words) are never needed by S1/S2 and only on ties by S3.
-__constant__ uint8_t c_block_order[15] = {12, 13, 14, 15, 16, 17, 2, 3, 6, 4, 5, 8, 9, 10, 11};
+// Blocks of one refill that the reference reads (16-byte block b = bytes 16b..16b+15):
+// 2, 3 (CDT high words of lanes 0..3, bytes 32..63), 4, 5, 6 (Bernoulli bytes 64..99),
+// 8..12 (CDT high words and Bernoulli bytes of lanes 4..7, 132..199), 12..17 (uniform words
+// from byte 200, sign byte 280).  Blocks 0, 1, 7 hold only the low CDT words, which S1/S2
+// never use and S3 uses only on ties (regenerated then).  kBufBlock lists them in buffer
+// order; word w of the refill (bytes 4w..4w+3) is buffer word kbuf(w).
+constexpr int kRefillBlocks = 15;
+__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17};
+__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : w - 12; }
 
-constexpr int kCandThreads = 384;  // 1 CTA (128 KiB of tables) per SM; 168 registers per thread
+constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
+constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed with p < 1e-7
 
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)
@@ -123,127 +124,56 @@ __global__ void __launch_bounds__(kCandThreads, 1)
       cur = st;
     }
     const uint32_t cb = t * 24u;
-    longlong2 *dst = reinterpret_cast<longlong2 *>(cand + (size_t)g * 8);
-    uint32_t U[22];
-    uint32_t keep0 = 0, keep1 = 0, k8 = 0, e6 = 0, carry = 0, acc = 0;
-    uint32_t y[8];
-    uint32_t x01 = 0, x23 = 0, x45 = 0, x67 = 0;  // CDT samples, two lanes per word
+    // 1. the keystream blocks, one AES body (keeps the loop inside the instruction cache)
+    uint4 buf4[kRefillBlocks];
 #pragma unroll 1
-    for (int bi = 0; bi < 15; ++bi) {
+    for (int bi = 0; bi < kRefillBlocks; ++bi) {
       uint32_t W[4];
-      aes256_ctr_block(W, 0u, cb + c_block_order[bi], rk, c);
-      // the pair of lanes completed by this block, if any
-      int lane0 = -1;
-      uint32_t xa = 0, xb = 0, ya = 0, yb = 0, ea = 0, eb = 0;
-      uint64_t ma = 0, mb = 0;
-      switch (bi) {
-        case 0:
-          keep0 = W[0];
-          keep1 = W[1];
-          U[0] = bswap32(W[2]);
-          U[1] = bswap32(W[3]);
-          break;
-        case 1: U[2] = bswap32(W[0]); U[3] = bswap32(W[1]); U[4] = bswap32(W[2]); U[5] = bswap32(W[3]); break;
-        case 2: U[6] = bswap32(W[0]); U[7] = bswap32(W[1]); U[8] = bswap32(W[2]); U[9] = bswap32(W[3]); break;
-        case 3: U[10] = bswap32(W[0]); U[11] = bswap32(W[1]); U[12] = bswap32(W[2]); U[13] = bswap32(W[3]); break;
-        case 4: U[14] = bswap32(W[0]); U[15] = bswap32(W[1]); U[16] = bswap32(W[2]); U[17] = bswap32(W[3]); break;
-        case 5: {
-          U[18] = bswap32(W[0]);
-          U[19] = bswap32(W[1]);
-          U[20] = bswap32(W[2]);
-          U[21] = bswap32(W[3]);
-          k8 = U[20] & 0xffu;
-          bool fast = true;
-#pragma unroll
-          for (int i = 0; i < 8; ++i) fast &= uniform_ok<SIG>(U[i]);
-          if (fast) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) y[i] = uniform_reduce<SIG>(U[i]);
-          } else {
-            uint32_t yl[8];
-            uniform_slow<SIG>(yl, cb, rkg, c, status);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) y[i] = yl[i];
-          }
-          break;
-        }
-        case 6:  // block 2: lanes 0, 1
-          x01 = cdt_lane<FULL>(0, le64_of(W[0], W[1]), cb, rkg, c) |
-                (cdt_lane<FULL>(1, le64_of(W[2], W[3]), cb, rkg, c) << 16);
-          break;
-        case 7:  // block 3: lanes 2, 3
-          x23 = cdt_lane<FULL>(2, le64_of(W[0], W[1]), cb, rkg, c) |
-                (cdt_lane<FULL>(3, le64_of(W[2], W[3]), cb, rkg, c) << 16);
-          break;
-        case 8:  // block 6: exponent bytes of lanes 0..3
-          e6 = W[0];
-          break;
-        case 9:  // block 4: lanes 0, 1
-          lane0 = 0;
-          xa = x01 & 0xffffu; xb = x01 >> 16; ya = y[0]; yb = y[1];
-          ma = le64_of(W[0], W[1]); mb = le64_of(W[2], W[3]);
-          ea = e6 >> 24; eb = (e6 >> 16) & 0xffu;
-          break;
-        case 10:  // block 5: lanes 2, 3
-          lane0 = 2;
-          xa = x23 & 0xffffu; xb = x23 >> 16; ya = y[2]; yb = y[3];
-          ma = le64_of(W[0], W[1]); mb = le64_of(W[2], W[3]);
-          ea = (e6 >> 8) & 0xffu; eb = e6 & 0xffu;
-          break;
-        case 11:  // block 8: lane 4 (132..139), first half of lane 5
-          x45 = cdt_lane<FULL>(4, le64_of(W[1], W[2]), cb, rkg, c);
-          carry = W[3];
-          break;
-        case 12:  // block 9: rest of lane 5, lane 6, first half of lane 7
-          x45 |= cdt_lane<FULL>(5, le64_of(carry, W[0]), cb, rkg, c) << 16;
-          x67 = cdt_lane<FULL>(6, le64_of(W[1], W[2]), cb, rkg, c);
-          carry = W[3];
-          break;
-        case 13:  // block 10: rest of lane 7 (CDT); mantissa of lane 4, half of lane 5
-          x67 |= cdt_lane<FULL>(7, le64_of(carry, W[0]), cb, rkg, c) << 16;
-          lane0 = 4;
-          xa = x45 & 0xffffu; ya = y[4];
-          ma = le64_of(W[1], W[2]);
-          ea = keep1 >> 24;
-          carry = W[3];
-          break;
-        case 14:  // block 11: rest of lane 5's mantissa, lanes 6 and 7 (7 ends in bytes 192..195)
-          lane0 = 5;
-          break;
-      }
-      if (bi == 14) {
-        // lanes 5, 6, 7 complete here
-        const uint64_t m5 = le64_of(carry, W[0]), m6 = le64_of(W[1], W[2]), m7 = le64_of(W[3], keep0);
-        uint64_t z5, z6, z7;
-        const bool b5 = candidate<SIG, VAR>(x45 >> 16, y[5], m5, (keep1 >> 16) & 0xffu, kinv, z5);
-        const bool b6 = candidate<SIG, VAR>(x67 & 0xffffu, y[6], m6, (keep1 >> 8) & 0xffu, kinv, z6);
-        const bool b7 = candidate<SIG, VAR>(x67 >> 16, y[7], m7, keep1 & 0xffu, kinv, z7);
-        acc |= (uint32_t)accept_final(b5, z5, (k8 >> 5) & 1u) << 5;
-        acc |= (uint32_t)accept_final(b6, z6, (k8 >> 6) & 1u) << 6;
-        acc |= (uint32_t)accept_final(b7, z7, (k8 >> 7) & 1u) << 7;
-        const int64_t v5 = ((k8 >> 5) & 1u) ? -(int64_t)z5 : (int64_t)z5;
-        const int64_t v6 = ((k8 >> 6) & 1u) ? -(int64_t)z6 : (int64_t)z6;
-        const int64_t v7 = ((k8 >> 7) & 1u) ? -(int64_t)z7 : (int64_t)z7;
-        // lane 4 was stored as the first half of pair (4, 5) in block 10
-        reinterpret_cast<int64_t *>(dst)[5] = v5;
-        dst[3] = make_longlong2(v6, v7);
-      } else if (lane0 >= 0) {
-        uint64_t za, zb = 0;
-        const bool ba = candidate<SIG, VAR>(xa, ya, ma, ea, kinv, za);
-        const uint32_t ka = (k8 >> lane0) & 1u;
-        acc |= (uint32_t)accept_final(ba, za, ka) << lane0;
-        const int64_t va = ka ? -(int64_t)za : (int64_t)za;
-        if (lane0 == 4) {
-          reinterpret_cast<int64_t *>(dst)[4] = va;
-        } else {
-          const bool bb = candidate<SIG, VAR>(xb, yb, mb, eb, kinv, zb);
-          const uint32_t kb = (k8 >> (lane0 + 1)) & 1u;
-          acc |= (uint32_t)accept_final(bb, zb, kb) << (lane0 + 1);
-          const int64_t vb = kb ? -(int64_t)zb : (int64_t)zb;
-          dst[lane0 >> 1] = make_longlong2(va, vb);
-        }
-      }
+      aes256_ctr_block(W, 0u, cb + c_refill_blocks[bi], rk, c);
+      buf4[bi] = make_uint4(W[0], W[1], W[2], W[3]);
     }
+    const uint32_t *buf = reinterpret_cast<const uint32_t *>(buf4);
+    // 2. uniform y: first 8 accepted words from byte 200 (src/gauss.c:578-703), branch-free
+    uint32_t y[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) y[j] = 0;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int w = 0; w < kUniformWords; ++w) {
+      const uint32_t v = bswap32(buf[kbuf(50 + w)]);
+      const bool ok = uniform_ok<SIG>(v) && cnt < 8;
+      const uint32_t r = uniform_reduce<SIG>(v);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) y[j] = (ok && cnt == (uint32_t)j) ? r : y[j];
+      cnt += ok ? 1u : 0u;
+    }
+    if (cnt < 8) uniform_slow<SIG>(y, cb, rkg, c, status);
+    uint32_t ybuf[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ybuf[j] = y[j];
+    const uint32_t k8 = bswap32(buf[kbuf(70)]) & 0xffu;  // sign byte 280
+    // 3. the 8 candidates, one code copy
+    uint32_t acc = 0;
+    int64_t v8[8];
+#pragma unroll 1
+    for (int ln = 0; ln < 8; ++ln) {
+      const int h = ln >> 2, li = ln & 3;
+      const int w2 = 25 * h + 8 + 2 * li;   // CDT high word of this lane (byte 32 + 8 li + 100 h)
+      const int wm = 25 * h + 16 + 2 * li;  // Bernoulli mantissa (byte 64 + 8 li + 100 h)
+      const int we = 25 * h + 24;           // exponent bytes (96 + 100 h)
+      const uint64_t r2 = le64_of(buf[kbuf(w2)], buf[kbuf(w2 + 1)]);
+      const uint32_t x = cdt_lane<FULL>(ln, r2, cb, rkg, c);
+      const uint64_t rm = le64_of(buf[kbuf(wm)], buf[kbuf(wm + 1)]);
+      const uint32_t rexp = (buf[kbuf(we)] >> (24 - 8 * li)) & 0xffu;
+      uint64_t z;
+      const bool b = candidate<SIG, VAR>(x, ybuf[ln], rm, rexp, kinv, z);
+      const uint32_t k = (k8 >> ln) & 1u;
+      acc |= (uint32_t)accept_final(b, z, k) << ln;
+      v8[ln] = k ? -(int64_t)z : (int64_t)z;
+    }
+    longlong2 *dst = reinterpret_cast<longlong2 *>(cand + (size_t)g * 8);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = make_longlong2(v8[2 * i], v8[2 * i + 1]);
     amask[g] = (uint8_t)acc;
   }
 }
