@@ -517,6 +517,7 @@ __global__ void __launch_bounds__(256) k_polya(const uint32_t *__restrict__ rkey
 
 // ------------------------------------------------------------------ host side
 
+
 static ModArgs mod_args() {
   ModArgs m;
   for (int j = 0; j < 3; ++j) {
@@ -620,8 +621,8 @@ uint32_t cpu_map_refills(uint32_t calls, uint32_t n, int sig) {
   return (R + 31) & ~31u;
 }
 
-int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
-                   uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s) {
+int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
+                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
   const uint32_t R = cpu_map_refills(calls, n, sig);
   const uint32_t tiles = (R + kScanTile - 1) / kScanTile;
   if ((uint64_t)nstreams * R >= (1ull << 32) - 1) return CUFE_ERR_INVALID;
@@ -641,25 +642,48 @@ int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t
   const uint32_t grid =
       (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (total + kCandThreads - 1) / kCandThreads);
   {
-  ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
-  if (sig == 0)
-    k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
-  else if (sig == 1)
-    k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
-  else
-    k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask, d_status);
+    ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
+    if (sig == 0)
+      k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
+                                                                         d_status);
+    else if (sig == 1)
+      k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
+                                                                         d_status);
+    else
+      k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
+                                                                        d_status);
   }
   CUFE_CUDA(cudaGetLastError());
-  { ProfScope ps("sample_scan", s);
-  k_scan_tiles<<<dim3(tiles, nstreams), 512, 0, s>>>(amask, R, tiles, elocal, tsum);
-  k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles); }
+  {
+    ProfScope ps("sample_scan", s);
+    k_scan_tiles<<<dim3(tiles, nstreams), 512, 0, s>>>(amask, R, tiles, elocal, tsum);
+    k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles);
+  }
   const uint32_t guess = (uint32_t)((double)n / mean_accept(sig));
-  { ProfScope ps("sample_walk", s);
-  k_walk<<<(nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, R, tiles, calls, n, guess, nstreams, cstart,
-                                            d_status); }
+  {
+    ProfScope ps("sample_walk", s);
+    k_walk<<<(nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, R, tiles, calls, n, guess, nstreams, cstart,
+                                              d_status);
+  }
+  CUFE_CUDA(cudaGetLastError());
+  out->cand = cand;
+  out->amask = amask;
+  out->call_start = cstart;
+  out->refills = R;
+  out->elocal = elocal;
+  out->tile_off = tsum;
+  out->tiles = tiles;
+  return CUFE_OK;
+}
+
+int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
+                   uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s) {
+  CpuMapCandidates cm;
+  int rc = sample_cpu_map_candidates(sig, nstreams, d_rkeys, calls, n, ws, d_status, num_sms, s, &cm);
+  if (rc) return rc;
   ProfScope ps_sc("sample_scatter", s);
-  k_scatter<<<dim3(calls, nstreams), 256, 0, s>>>(cand, amask, elocal, tsum, cstart, R, tiles, calls, n, mod_args(),
-                                                  d_out);
+  k_scatter<<<dim3(calls, nstreams), 256, 0, s>>>(cm.cand, cm.amask, cm.elocal, cm.tile_off, cm.call_start,
+                                                  cm.refills, cm.tiles, calls, n, mod_args(), d_out);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }

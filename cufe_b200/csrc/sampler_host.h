@@ -24,6 +24,23 @@ size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, in
 int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
                    uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s);
 
+// The candidate form of the CPU mapping, for consumers that gather the samples themselves:
+// cand[stream][refill][8] signed candidates, amask[stream][refill] accept bits and
+// call_start[stream][calls+1] (refill index where each call starts; the last entry is the
+// end of the last call).  Sample j of call c is the j-th accepted candidate of refills
+// call_start[c] .. call_start[c+1]-1, in order.
+struct CpuMapCandidates {
+  const int64_t *cand;
+  const uint8_t *amask;
+  const uint32_t *call_start;
+  uint32_t refills;  // per stream
+  // per-stream exclusive prefix of accept counts: elocal[t] + tile_off[t / 4096]
+  const uint32_t *elocal, *tile_off;
+  uint32_t tiles;
+};
+int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
+                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out);
+
 // GPU counter mapping: polynomials poly0 .. poly0+npolys-1 of one key, residues to
 // d_out[npolys][3][n].
 int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npolys, uint32_t n,

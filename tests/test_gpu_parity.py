@@ -4,6 +4,10 @@ The oracle (oracle/cufe_oracle.c) is pinned bit-for-bit to the reference's own C
 (tests/test_oracle.py); residues are compared canonically (the reference's mod_prime may
 return q_j for 0).
 """
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -92,7 +96,7 @@ def test_sampler_gpu_map(sig, rng, oracle_built):
         assert (got[p] == canon(O.gauss_modeB(rk, sig, 2 + p))).all(), (sig, p)
 
 
-@pytest.mark.parametrize("n,l", [(256, 8), (1024, 16), (2048, 124)])
+@pytest.mark.parametrize("n,l", [(256, 8), (1024, 16), (2048, 124), (4096, 16), (8192, 8)])
 def test_scheme_cpu_map(n, l, rng, oracle_built):
     c = cf.Context(n, l)
     O = Oracle(n, l)
@@ -132,6 +136,32 @@ def test_scheme_cpu_map(n, l, rng, oracle_built):
             rdec = O.decode(rdy)
             assert (dec[b * 2 + k] == rdec).all()
             assert int(rdec[0]) == int(x[b].astype(np.int64) @ y[k].astype(np.int64))
+
+
+def test_c2_shape_golden_hashes():
+    """setup / encrypt / keygen / decrypt / decode at n = 4096, l = 784 against the SHA-256 of
+    the reference CPU build's outputs for the same seeds (tests/golden/ref_c2.json)"""
+    doc = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_c2.json")))
+    n, l = doc["n"], doc["l"]
+    rng = np.random.default_rng(0xC0FE0002)
+    seed_a, seed_e, seed2 = rng.integers(0, 256, (3, 32), dtype=np.uint8)
+    x = rng.integers(0, 5, l, dtype=np.uint32)
+    y = rng.integers(0, 17, l, dtype=np.uint32)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    c = cf.Context(n, l)
+    mpk, msk = c.setup(seed_a, None, seed_e)
+    ct = c.encrypt(dev(x[None]), mpk, seed2[None], None)
+    sky = c.keygen(dev(y[None]), msk)
+    dy = c.decrypt(ct, dev(y[None]), sky)
+    dec = c.decode(dy)
+    c.sync()
+    assert sha(cf.u32(mpk)) == doc["mpk"] and sha(cf.u32(msk)) == doc["msk"]
+    assert sha(cf.u32(ct)[0]) == doc["ct"]
+    assert sha(cf.u32(sky)[0]) == doc["sky"]
+    assert sha(cf.u32(dy)[0, 0]) == doc["dy"]
+    d = cf.u32(dec)
+    assert sha(d[0]) == doc["dec"] and int(d[0][0]) == doc["ip"]
+    c.close()
 
 
 def test_scheme_gpu_map(rng, oracle_built):
