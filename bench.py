@@ -8,6 +8,12 @@ encrypt(x) + keygen(y) (one key, done once) + decrypt + decode of all N coeffici
 inner product is coefficient 0, centred.  A step is one batch of B encryptions through the
 whole pipeline; the batch output is checked against the plaintext dot products after timing.
 
+Besides the batched value the line carries: "plain" (one encryption per call, device-resident,
+the same kernels), "plain_dropin" (the reference's per-call form through the four
+rlwe_sife_*_gpu symbols on host buffers), "coef0" (batched with the constant-coefficient
+decrypt), "e2e" (batched through the C ABI with pinned host inputs and results), the roofline
+of the dominant kernel and the clocks sampled during the timed region.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl cufe|reference]
 
 --impl reference times the reference's own CPU implementation (cuFE src/*.c compiled from
@@ -200,6 +206,13 @@ def cpu_baseline_sample(x, y, seeds2, setup_seeds, nproc, steps=2):
 
 # ----------------------------------------------------------------------------- GPU arm
 
+# DRAM bytes per refill of the sigma_3 candidate kernel, from one ncu capture of a batch-16
+# launch (dram__bytes_read.sum + dram__bytes_write.sum = 3.71 MB + 1402.23 MB over
+# 16 x 1,103,616 refills); traffic grows with the refill count, so a launch of B streams
+# moves B x refills x this
+CAND_S3_DRAM_BYTES_PER_REFILL = (3.708416e6 + 1402.233648e6) / (16 * 1103616)
+
+
 # algorithmic HBM bytes per launch of each kernel at this workload (batch B)
 def algorithmic_bytes(kernel, B, refills3):
     poly = 3 * N * 4
@@ -210,6 +223,61 @@ def algorithmic_bytes(kernel, B, refills3):
         "decrypt": B * (L + 1) * poly + B * poly,        # ciphertexts read, d_y written
         "decode": B * poly + B * N * 4,
     }.get(kernel)
+
+
+def crt_decode(v, p):
+    """Garner CRT of one coefficient's three residues and the reference's rounding
+    (crt_reverse_gmp + round_extract_gmp2, src/crt.c:46-81, src/rlwe_sife.c:334-393): the
+    caller-side host decode of the drop-in form"""
+    from cufe_b200 import Q
+    q = Q[0] * Q[1] * Q[2]
+    x = 0
+    for j in range(3):
+        mj = q // Q[j]
+        x += int(v[j]) * mj * pow(mj, -1, Q[j])
+    x %= q
+    quo, rem = divmod(p * x, q)
+    return quo + (1 if rem > q // 2 else 0)
+
+
+def dropin_plain(cf, ctx, mpk, msk, x, y, seeds2, calls, device):
+    """The reference's plain per-call GPU form: per inner product one rlwe_sife_encrypt_gpu
+    (repeat 1) and one rlwe_sife_decrypt_gmp_gpu (two keys: y+ and y-, since the reference
+    reduces y as uint32) on host buffers, synchronous, then the host decode of coefficient 0.
+    Keys come from one rlwe_sife_keygen_gpu call made before timing."""
+    import ctypes as C
+    L_ = cf.lib()
+    if L_.cufe_dropin_configure(N, L, device) != 0:
+        return {"value": None, "error": "cufe_dropin_configure failed"}
+    mpk_h = np.ascontiguousarray(cf.u32(mpk))
+    msk_h = np.ascontiguousarray(cf.u32(msk))
+    yv = y[0].astype(np.int64)
+    ys = np.stack([np.where(yv > 0, yv, 0), np.where(yv < 0, -yv, 0)]).astype(np.uint32)
+    sk = np.zeros((2, 3, N), np.uint32)
+    L_.rlwe_sife_keygen_gpu(ys.ctypes.data, msk_h.ctypes.data, sk.ctypes.data, 2, None)
+    ct = np.zeros((L + 1, 3, N), np.uint32)
+    dy = np.zeros((2, 3, N), np.uint32)
+    p = 64 * L + 1
+    lat, ok = [], True
+    for i in range(calls + 2):
+        xi = np.ascontiguousarray(x[i])
+        s2 = np.ascontiguousarray(seeds2[i])
+        t0 = time.perf_counter()
+        L_.rlwe_sife_encrypt_gpu(xi.ctypes.data, mpk_h.ctypes.data, ct.ctypes.data, s2.ctypes.data, s2.ctypes.data, 1,
+                                 None)
+        L_.rlwe_sife_decrypt_gmp_gpu(ct.ctypes.data, ys.ctypes.data, sk.ctypes.data, dy.ctypes.data, 2, None)
+        v = (crt_decode(dy[0, :, 0], p) - crt_decode(dy[1, :, 0], p)) % p
+        t1 = time.perf_counter()
+        v = v - p if v > p // 2 else v
+        ok = ok and v == int(x[i].astype(np.int64) @ yv)
+        if i >= 2:
+            lat.append(1000.0 * (t1 - t0))
+    ok = ok and L_.cufe_dropin_status() == 0
+    return {"value": 1000.0 * len(lat) / sum(lat), "unit": UNIT, "calls": len(lat),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)), "bit_exact": ok,
+            "form": "reference per-call form: rlwe_sife_encrypt_gpu (repeat 1) + rlwe_sife_decrypt_gmp_gpu "
+                    "(2 keys) on pageable host buffers, synchronous, host decode of coefficient 0; GPU counter "
+                    "mapping; wall clock"}
 
 
 def gpu_arm(args):
@@ -299,6 +367,26 @@ def gpu_arm(args):
              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
              "form": "one encryption per call (batch 1), device-resident, same kernels"}
 
+    # --- batched with the constant-coefficient decrypt (decrypt + decode of coefficient 0 only)
+    r0 = torch.empty((steps, B, 1), dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for k in range(steps):
+        b0 = ((warm + k) % nb) * B
+        ctx.encrypt(x_dev[b0:b0 + B], mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
+        ctx.decrypt_coef0(ct, y_dev, sky, y_signed=True, out=r0[k])
+    g1.record(stream)
+    torch.cuda.synchronize()
+    c0_ms = max_over_ranks(g0.elapsed_time(g1), dev)
+    g = cf.u32(r0[:, :, 0]).astype(np.int64)
+    coef0 = {"value": steps * B * world / (c0_ms / 1000.0), "unit": UNIT, "ms_per_step": c0_ms / steps,
+             "bit_exact": bool((np.where(g > p // 2, g - p, g) == exp).all()),
+             "form": "batched, decrypt and decode of coefficient 0 only (the coefficient the reference decodes)"}
+
+    # --- the reference's plain per-call GPU form, through the drop-in symbols
+    plain_dropin = dropin_plain(cf, ctx, mpk, msk, x, y, seeds2, args.dropin_calls, local)
+
     # --- end to end through the C ABI with host buffers (pinned), copies in the timed region
     xh = torch.from_numpy(x.view(np.int32)).pin_memory()
     rh = torch.empty((steps, B), dtype=torch.int32).pin_memory()
@@ -339,7 +427,9 @@ def gpu_arm(args):
     abytes = algorithmic_bytes(name, B, refills3)
     roof = {"kernel": name, "bound": "hbm", "unit": "GB/s", "peak": hbm_peak,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "achieved": (abytes / per_launch_s / 1e9) if abytes else None, "traffic": None,
+            "achieved": (abytes / per_launch_s / 1e9) if abytes else None,
+            "traffic": (CAND_S3_DRAM_BYTES_PER_REFILL * refills3 * B) if name == "sample_cand_s3" else None,
+            "algorithmic_bytes": abytes,
             "share": tot / sum(v[1] for v in prof.values())}
     roof["frac"] = roof["achieved"] / hbm_peak if roof["achieved"] else None
     if name.startswith("sample_cand"):
@@ -362,6 +452,9 @@ def gpu_arm(args):
                        "randomness": "CPU stream mapping, every stream keyed by a per-encryption seed"},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
             "plain": plain, "batched_vs_plain": ips / world / plain["value"],
+            "plain_dropin": plain_dropin,
+            "batched_vs_plain_dropin": ips / world / plain_dropin["value"] if plain_dropin.get("value") else None,
+            "coef0": coef0,
             "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "clocks": clocks}
@@ -387,6 +480,7 @@ def main():
     ap.add_argument("--batch", type=int, default=200)
     ap.add_argument("--impl", default="cufe", choices=["cufe", "reference"])
     ap.add_argument("--plain-calls", type=int, default=30)
+    ap.add_argument("--dropin-calls", type=int, default=20)
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -62,6 +62,7 @@ def lib():
             "cufe_decrypt": [vp, i, vp, i, vp, i, vp, vp, vp],
             "cufe_decrypt_noalloc": [vp, vp, i, vp, i, vp, vp, vp],
             "cufe_decode": [vp, i, vp, i, vp, vp],
+            "cufe_decrypt_coef0": [vp, i, vp, i, vp, i, vp, vp, vp, vp],
             "cufe_sample_cpu_map": [vp, i, i, vp, i, vp, vp],
             "cufe_sample_gpu_map": [vp, i, vp, i, i, vp, vp],
             "cufe_sample_polya": [vp, vp, vp, vp],
@@ -257,6 +258,14 @@ class Context:
         _check(lib().cufe_decrypt_noalloc(self.h, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(dy),
                                           _stream(stream, self.device)), "cufe_decrypt_noalloc")
         return dy
+
+    def decrypt_coef0(self, ct, y, sky, y_signed=False, d0=None, out=None, stream=None):
+        """decrypt and decode coefficient 0 of every (ciphertext, key) pair: out[nct][nkeys]"""
+        nct, nkeys = ct.shape[0], y.shape[0]
+        out = _dev((nct, nkeys), self.dev) if out is None else out
+        _check(lib().cufe_decrypt_coef0(self.h, nct, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(d0),
+                                        _ptr(out), _stream(stream, self.device)), "cufe_decrypt_coef0")
+        return out
 
     def decode(self, dy, ncoeff=None, out=None, stream=None):
         ncoeff = self.n if ncoeff is None else ncoeff

@@ -193,6 +193,12 @@ int cufe_decrypt_noalloc(cufe_ctx *h, const uint32_t *d_ct, int nkeys, const uin
   CTX_CALL(h, cufe::ctx_decrypt_noalloc(h->c, d_ct, nkeys, d_y, y_signed, d_sky, d_dy, h->c.pick(stream)));
 }
 
+int cufe_decrypt_coef0(cufe_ctx *h, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                       const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, void *stream) {
+  if (!d_ct || !d_y || !d_sky || !d_out) return CUFE_ERR_INVALID;
+  CTX_CALL(h, cufe::ctx_decrypt_coef0(h->c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d_d0, d_out, h->c.pick(stream)));
+}
+
 int cufe_decode(cufe_ctx *h, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, void *stream) {
   if (!d_dy || !d_out) return CUFE_ERR_INVALID;
   CTX_CALL(h, cufe::ctx_decode(h->c, count, d_dy, ncoeff, d_out, h->c.pick(stream)));

@@ -71,6 +71,8 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
 int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                         const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s);
 int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s);
+int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                      const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s);
 int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
                        cudaStream_t s);
 int ctx_sample_gpu_map(Ctx &c, int sig, const uint8_t *key, int poly0, int npolys, uint32_t *d_out,

@@ -481,13 +481,7 @@ struct DecodeArgs {
 
 // crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332): Garner
 // to x in [0, q), then floor(p x / q) + (remainder > floor(q/2)).
-__global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff, uint32_t *__restrict__ out,
-                         DecodeArgs d) {
-  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (long long)count * ncoeff) return;
-  const int cnt = (int)(gid / ncoeff), k = (int)(gid - (long long)cnt * ncoeff);
-  const uint32_t *v = dy + (size_t)cnt * 3 * d.n + k;
-  const uint32_t v0 = v[0], v1 = v[d.n], v2 = v[2 * (size_t)d.n];
+__device__ __forceinline__ uint32_t decode_one(uint32_t v0, uint32_t v1, uint32_t v2, const DecodeArgs &d) {
   const uint32_t t1 = mod_red1(v1 + d.q1 - v0 % d.q1, d.q1);
   const uint32_t u1 = shoup_mul(t1, d.c1, d.c1_sh, d.q1);
   const uint64_t x1 = (uint64_t)v0 + (uint64_t)d.q0 * u1;
@@ -511,7 +505,70 @@ __global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff,
     rem -= Q;
   }
   if (rem > H) ++qe;
-  out[gid] = (uint32_t)qe;
+  return (uint32_t)qe;
+}
+
+__global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff, uint32_t *__restrict__ out,
+                         DecodeArgs d) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)count * ncoeff) return;
+  const int cnt = (int)(gid / ncoeff), k = (int)(gid - (long long)cnt * ncoeff);
+  const uint32_t *v = dy + (size_t)cnt * 3 * d.n + k;
+  out[gid] = decode_one(v[0], v[d.n], v[2 * (size_t)d.n], d);
+}
+
+// sum over the CTA of one u64 per thread (values < 2^40); red: blockDim.x/32 words
+__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, uint64_t *red) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint64_t t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Constant-coefficient decryption and decode.  The reference decodes only coefficient 0 of
+// d_y (src/rlwe_sife.c:380, main.c:205 and 326), so per (ciphertext, key) and modulus
+//   d_y[0] = sum_i y_i c_i[0] - (c_l * sk_y)[0],
+//   (c_l * sk_y)[0] = c_l[0] sk_y[0] - sum_{t=1}^{n-1} c_l[t] sk_y[n-t]   (negacyclic),
+// equal to coefficient 0 of the full decryption (src/rlwe_sife.c:248-286) residue for residue.
+// One CTA per (ciphertext, key); reads l + 2n words per modulus instead of (l+1) n.
+__global__ void __launch_bounds__(256)
+    k_dec_coef0(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ y, int y_signed, int nkeys,
+                const uint32_t *__restrict__ sky, uint32_t *__restrict__ d0, uint32_t *__restrict__ out,
+                SchemeArgs sa, DecodeArgs dd) {
+  __shared__ uint64_t red[8];
+  const int n = sa.ra.n, l = sa.l;
+  const int key = blockIdx.x % nkeys, c = blockIdx.x / nkeys;
+  const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * n;
+  uint32_t r[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const uint32_t q = sa.ra.q[m];
+    const uint64_t mu = sa.mu[m];
+    uint64_t mac = 0, neg = 0;
+    for (int i = threadIdx.x; i < l; i += blockDim.x) {
+      const uint32_t yv = y_residue(y[(size_t)key * l + i], y_signed, q, mu);
+      mac += mod_u64((uint64_t)cb[((size_t)i * 3 + m) * n] * yv, mu, q);
+    }
+    const uint32_t *cl = cb + ((size_t)l * 3 + m) * n;
+    const uint32_t *sk = sky + ((size_t)key * 3 + m) * n;
+    for (int t = threadIdx.x + 1; t < n; t += blockDim.x) neg += mod_u64((uint64_t)cl[t] * sk[n - t], mu, q);
+    const uint64_t macs = block_sum_u64(mac, red), negs = block_sum_u64(neg, red);
+    const uint32_t c0s0 = mod_u64((uint64_t)cl[0] * sk[0], mu, q);
+    // mac - (c_l[0] s[0] - neg)
+    r[m] = mod_add(mod_sub(mod_u64(macs, mu, q), c0s0, q), mod_u64(negs, mu, q), q);
+  }
+  if (threadIdx.x == 0) {
+    if (d0) {
+      d0[(size_t)blockIdx.x * 3 + 0] = r[0];
+      d0[(size_t)blockIdx.x * 3 + 1] = r[1];
+      d0[(size_t)blockIdx.x * 3 + 2] = r[2];
+    }
+    out[blockIdx.x] = decode_one(r[0], r[1], r[2], dd);
+  }
 }
 
 }  // namespace
@@ -948,8 +1005,7 @@ int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t 
   });
 }
 
-int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s) {
-  if (count < 1 || ncoeff < 1 || ncoeff > c.n) return CUFE_ERR_INVALID;
+static DecodeArgs decode_args(const Ctx &c) {
   DecodeArgs d;
   d.q0 = kRefPrimes[0];
   d.q1 = kRefPrimes[1];
@@ -966,9 +1022,25 @@ int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_
   d.hhi = (unsigned long long)(uint64_t)(c.qhalf >> 64);
   d.p = c.p;
   d.n = c.n;
+  return d;
+}
+
+int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s) {
+  if (count < 1 || ncoeff < 1 || ncoeff > c.n) return CUFE_ERR_INVALID;
+  const DecodeArgs d = decode_args(c);
   const long long total = (long long)count * ncoeff;
   ProfScope ps("decode", s);
   k_decode<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_dy, count, ncoeff, d_out, d);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                      const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s) {
+  if (nct < 1 || nkeys < 1 || (long long)nct * nkeys > 0x7fffffffLL || !d_out) return CUFE_ERR_INVALID;
+  ProfScope ps("decrypt_coef0", s);
+  k_dec_coef0<<<(unsigned)(nct * nkeys), 256, 0, s>>>(d_ct, d_y, y_signed, nkeys, d_sky, d_d0, d_out,
+                                                      scheme_args(c), decode_args(c));
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }

@@ -137,6 +137,14 @@ int cufe_decrypt_noalloc(cufe_ctx *ctx, const uint32_t *d_ct, int nkeys, const u
 /* crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332) on the first
  * ncoeff coefficients of each of count d_y: d_out[count][ncoeff], values in [0, p] */
 int cufe_decode(cufe_ctx *ctx, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, void *stream);
+/* Decrypt and decode coefficient 0 only, the one coefficient the reference reads after
+ * decryption (src/rlwe_sife.c:380; main.c:205, 326).  For every (ciphertext, key) pair:
+ * d_out[nct][nkeys] = decode of d_y[0], where d_y[0] = sum_i y_i c_i[0] - (c_l * sk_y)[0] with
+ * the negacyclic constant term (c_l * sk_y)[0] = c_l[0] sk_y[0] - sum_{t>=1} c_l[t] sk_y[n-t].
+ * Equal to cufe_decode(cufe_decrypt(...), ncoeff = 1).  d_d0 (optional, may be NULL) receives
+ * the residues d_d0[nct][nkeys][3]. */
+int cufe_decrypt_coef0(cufe_ctx *ctx, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                       const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, void *stream);
 
 /* samplers, for parity tests and statistics.  CPU mapping: nstreams AES-CTR streams keyed by
  * keys[nstreams][32] (NULL: zero-key streams), each running `calls` consecutive

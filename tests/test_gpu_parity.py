@@ -164,6 +164,45 @@ def test_c2_shape_golden_hashes():
     c.close()
 
 
+@pytest.mark.parametrize("n,l", [(256, 8), (2048, 124), (4096, 784)])
+def test_decrypt_coef0(n, l, rng, oracle_built):
+    """the constant-coefficient decrypt equals coefficient 0 of the full decrypt and its decode,
+    for uint32 (reference) and signed y; at n = 256 also the oracle's decrypt"""
+    c = cf.Context(n, l)
+    sa, se = seeds(rng, 2)
+    mpk, msk = c.setup(sa, None, se)
+    B, K = 3, 4
+    x = rng.integers(0, 5, (B, l), dtype=np.uint32)
+    s2 = seeds(rng, B)
+    ct = c.encrypt(dev(x), mpk, s2, None)
+    p = 64 * l + 1
+    for signed in (False, True):
+        if signed:
+            yi = rng.integers(-16, 17, (K, l), dtype=np.int64)
+            y = yi.astype(np.int32).view(np.uint32)
+        else:
+            y = rng.integers(0, 17, (K, l), dtype=np.uint32)
+            yi = y.astype(np.int64)
+        yd = dev(y)
+        sky = c.keygen(yd, msk, y_signed=signed)
+        dy = c.decrypt(ct, yd, sky, y_signed=signed)
+        full = cf.u32(c.decode(dy, ncoeff=1)).reshape(B, K)
+        d0 = dev(np.zeros((B, K, 3), np.uint32))
+        got = cf.u32(c.decrypt_coef0(ct, yd, sky, y_signed=signed, d0=d0))
+        c.sync()
+        assert (cf.u32(d0) == cf.u32(dy)[:, :, :, 0]).all()
+        assert (got == full).all()
+        assert (got.astype(np.int64) % p == (x.astype(np.int64) @ yi.T) % p).all()
+        if n == 256 and not signed:
+            O = Oracle(n, l)
+            rmpk, rmsk = O.setup(sa, None, se)
+            for b in range(B):
+                rct = O.encrypt(x[b], rmpk, s2[b], None)
+                for k in range(K):
+                    assert int(got[b, k]) == int(O.decode(O.decrypt(rct, y[k], O.keygen(y[k], rmsk)))[0])
+    c.close()
+
+
 def test_scheme_gpu_map(rng, oracle_built):
     n, l = 1024, 16
     c = cf.Context(n, l)
