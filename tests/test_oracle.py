@@ -137,3 +137,26 @@ def test_random_cases_against_reference_build(oracle_built):
     for sig in range(3):
         key = rng.integers(0, 256, 32, dtype=np.uint8)
         assert (R.gauss(sig, key, 20) == O.gauss(sig, key, 20)[0]).all()
+
+
+def test_sampler_shapes(oracle_built):
+    """pins what the reference's samplers draw: sigma_1 is D_{Z,sigma_1}; sigma_2 and sigma_3
+    are not (their Bernoulli input conversion is exact only below 2^52), with standard
+    deviations 1.13 and 0.73 of K sigma_0"""
+    import torch
+    from cufe_b200.stats import ChiSquare, sigma_of, signed_samples
+    O = Oracle(1024, 8)
+    rng = np.random.default_rng(0xC0FE0004)
+    ratios = []
+    for sig in range(3):
+        acc = ChiSquare(sigma_of(sig), 100)
+        xs = []
+        for _ in range(8):
+            r, _ = O.gauss(sig, rng.integers(0, 256, 32, dtype=np.uint8), 32)
+            x = signed_samples(torch.from_numpy(r.view(np.int32)))
+            acc.add(x)
+            xs.append(x.numpy())
+        ratios.append(float(np.concatenate(xs).astype(np.float64).std() / sigma_of(sig)))
+        p = acc.result()["p_value"]
+        assert (p > 1e-6) if sig == 0 else (p < 1e-12), (sig, p)
+    assert abs(ratios[0] - 1) < 0.01 and abs(ratios[1] - 1.13) < 0.02 and abs(ratios[2] - 0.73) < 0.02, ratios
