@@ -485,7 +485,8 @@ def ntt_sweep(args):
     """Negacyclic NTT and INTT over 65,536 polynomials x n in {1024..8192} x k in {3..6} RNS
     primes (the three params.h primes, then primes 1 mod 16384 below 2^31), residues uniform
     in [0, q_j) from seed 0xC0FE0004.  Each pass reads and writes every residue once: 8n
-    bytes per residue polynomial.  Every buffer is larger than L2 except n=1024, k=3 at
+    bytes per residue polynomial.  All three kernel variants are timed; the reported figure is
+    the one the ring's tuner (cufe_ring_tune) picks.  Every buffer is larger than L2 except n=1024, k=3 at
     fewer polynomials; each timed forward is followed by its inverse and the data must
     come back unchanged."""
     import torch
@@ -507,26 +508,36 @@ def ntt_sweep(args):
                 data[:, j, :] = torch.randint(0, int(ring.primes[j]), (npoly, n), generator=g, device=dev,
                                               dtype=torch.int64).to(torch.int32)
             orig = data.clone()
-            for _ in range(args.warmup):
-                ring.forward(data)
-                ring.inverse(data)
-            fwd, inv = [], []
-            for _ in range(args.steps):
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-                ev[0].record(stream)
-                ring.forward(data)
-                ev[1].record(stream)
-                ring.inverse(data)
-                ev[2].record(stream)
-                torch.cuda.synchronize()
-                fwd.append(ev[0].elapsed_time(ev[1]))
-                inv.append(ev[1].elapsed_time(ev[2]))
-            ok = bool(torch.equal(data, orig))
             nbytes = 8 * n * npoly * k
-            f_ms, i_ms = float(np.median(fwd)), float(np.median(inv))
+            per_variant = {}
+            ok = True
+            for var in (1, 2, 3):
+                ring.set_variant(var, var)
+                for _ in range(args.warmup):
+                    ring.forward(data)
+                    ring.inverse(data)
+                fwd, inv = [], []
+                for _ in range(args.steps):
+                    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                    ev[0].record(stream)
+                    ring.forward(data)
+                    ev[1].record(stream)
+                    ring.inverse(data)
+                    ev[2].record(stream)
+                    torch.cuda.synchronize()
+                    fwd.append(ev[0].elapsed_time(ev[1]))
+                    inv.append(ev[1].elapsed_time(ev[2]))
+                ok = ok and bool(torch.equal(data, orig))
+                per_variant[var] = (float(np.median(fwd)), float(np.median(inv)))
+            tuned = ring.tune(npoly)
+            fv, iv = tuned["variant"]
+            f_ms, i_ms = per_variant[fv][0], per_variant[iv][1]
             rows.append({"n": n, "k": k, "bytes_per_pass": nbytes, "fwd_ms": f_ms, "inv_ms": i_ms,
                          "fwd_gbs": nbytes / f_ms / 1e6, "inv_gbs": nbytes / i_ms / 1e6,
                          "fwd_frac": nbytes / f_ms / 1e6 / peak, "inv_frac": nbytes / i_ms / 1e6 / peak,
+                         "tuned_variant": [fv, iv],
+                         "variants_gbs": {str(v): [nbytes / t[0] / 1e6, nbytes / t[1] / 1e6]
+                                          for v, t in per_variant.items()},
                          "roundtrip_ok": ok, "primes": [int(q) for q in ring.primes]})
             del data, orig
             ring.close()

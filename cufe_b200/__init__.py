@@ -71,6 +71,9 @@ def lib():
             "cufe_ring_info": [vp, vp, vp, vp, vp],
             "cufe_ntt_forward": [vp, vp, ll, vp],
             "cufe_ntt_inverse": [vp, vp, ll, vp],
+            "cufe_ring_tune": [vp, ll, vp, vp],
+            "cufe_ring_set_variant": [vp, i, i],
+            "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
             "cufe_dropin_configure": [i, i, i],
             "cufe_dropin_status": [],
@@ -333,3 +336,19 @@ class Ring:
         npoly = data.numel() // (self.k * self.n)
         _check(lib().cufe_ntt_inverse(self.h, _ptr(data), npoly, _stream(stream, self.device)), "cufe_ntt_inverse")
         return data
+
+    def tune(self, npoly, stream=None):
+        """time the three kernel variants in both directions on npoly scratch polynomials and
+        keep the fastest; returns {"fwd": [ms v1, v2, v3], "inv": [...], "variant": (fwd, inv)}"""
+        ms = np.zeros(6, np.float32)
+        _check(lib().cufe_ring_tune(self.h, npoly, ms.ctypes.data, _stream(stream, self.device)), "cufe_ring_tune")
+        return {"fwd": [float(x) for x in ms[:3]], "inv": [float(x) for x in ms[3:]], "variant": self.variant}
+
+    @property
+    def variant(self):
+        f, v = C.c_int(0), C.c_int(0)
+        _check(lib().cufe_ring_get_variant(self.h, C.byref(f), C.byref(v)), "cufe_ring_get_variant")
+        return f.value, v.value
+
+    def set_variant(self, fwd, inv):
+        _check(lib().cufe_ring_set_variant(self.h, fwd, inv), "cufe_ring_set_variant")

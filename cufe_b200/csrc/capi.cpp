@@ -281,6 +281,26 @@ int cufe_ntt_inverse(const cufe_ring *h, uint32_t *d_data, long long npoly, void
   return cufe::ntt_launch(h->r.args, d_data, npoly * h->r.k, true, static_cast<cudaStream_t>(stream));
 }
 
+int cufe_ring_tune(cufe_ring *h, long long npoly, float *ms, void *stream) {
+  if (!h || npoly < 1) return CUFE_ERR_INVALID;
+  if (cudaSetDevice(h->r.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return cufe::ring_tune(h->r, npoly, ms, static_cast<cudaStream_t>(stream));
+}
+
+int cufe_ring_set_variant(cufe_ring *h, int fwd, int inv) {
+  if (!h || fwd < 1 || fwd > 3 || inv < 1 || inv > 3) return CUFE_ERR_INVALID;
+  h->r.args.pp_fwd = fwd;
+  h->r.args.pp_inv = inv;
+  return CUFE_OK;
+}
+
+int cufe_ring_get_variant(const cufe_ring *h, int *fwd, int *inv) {
+  if (!h) return CUFE_ERR_INVALID;
+  if (fwd) *fwd = h->r.args.pp_fwd;
+  if (inv) *inv = h->r.args.pp_inv;
+  return CUFE_OK;
+}
+
 // ------------------------------------------------------------------ reference drop-in
 
 namespace {

@@ -19,7 +19,7 @@ struct Ring {
   int device = 0, n = 0, logn = 0, k = 0;
   std::vector<uint32_t> q, psi_root;       // primes and the primitive 2n-th roots used
   std::vector<uint32_t> h_psi, h_ipsi;     // host copies [k][n] (bit-reversed powers)
-  uint32_t *d_tab = nullptr;               // psi, psi_sh, ipsi, ipsi_sh: 4 x [k][n]
+  uint32_t *d_tab = nullptr;               // psi2, ipsi2: 2 x [k][n] (w, w_shoup) pairs
   RingArgs args{};
   int init(int n, int k, const uint32_t *primes, int device);
   void release();
@@ -55,6 +55,9 @@ struct Ctx {
 
 int ntt_launch(const RingArgs &ra, uint32_t *data, long long nres, bool inverse, cudaStream_t s);
 int ntt_fwd_shoup_launch(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s);
+// times the NTT variants on npoly scratch polynomials, keeps the fastest per direction in
+// r.args; ms[4] (optional): {fwd v1, fwd v2, inv v1, inv v2}
+int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s);
 
 int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,
                       uint32_t *d_msk, cudaStream_t s);

@@ -18,26 +18,31 @@ constexpr int kMaxLogN = 13;
 
 // Device-visible description of an RNS ring Z_q[X]/(X^n+1): the primes and the
 // bit-reversed twiddle tables (psi[m+i] = psi^{bitrev(m+i)}, the layout of the
-// reference's consts.h) with their Shoup companions floor(w * 2^32 / q).
+// reference's consts.h), each entry interleaved with its Shoup companion
+// floor(w * 2^32 / q) so that one 8- or 16-byte load fetches one or two twiddles.
 struct RingArgs {
   int n, logn, k;
   uint32_t q[kMaxModuli];
   uint32_t ninv[kMaxModuli], ninv_sh[kMaxModuli];  // n^-1
   uint32_t w1n[kMaxModuli], w1n_sh[kMaxModuli];    // psi_inv[1] * n^-1 (last inverse stage)
-  const uint32_t *psi, *psi_sh, *ipsi, *ipsi_sh;   // [k][n] each
+  const uint2 *psi2, *ipsi2;                       // [k][n] (w, w_shoup) each
+  int pp_fwd, pp_inv;  // NTT kernel variant per direction (1, 2, 3), set by the tuner
 };
 
 // ------------------------------------------------------------------ arithmetic
 // All residues are kept canonical in [0, q) with q < 2^31.
 
+// The reductions are min(x, x - q) over uint32 (x - q wraps above x when x < q), written
+// with the fused add-and-min __viaddmin_u32(a, b, c) = min(a + b, c).
 __device__ __forceinline__ uint32_t mod_red1(uint32_t x, uint32_t q) {  // x < 2q
-  return min(x, x - q);
+  return __viaddmin_u32(x, 0u - q, x);
 }
-__device__ __forceinline__ uint32_t mod_add(uint32_t a, uint32_t b, uint32_t q) {
-  return mod_red1(a + b, q);
+__device__ __forceinline__ uint32_t mod_add(uint32_t a, uint32_t b, uint32_t q) {  // a, b < q
+  return __viaddmin_u32(a, b, a + b - q);
 }
-__device__ __forceinline__ uint32_t mod_sub(uint32_t a, uint32_t b, uint32_t q) {
-  return mod_red1(a - b + q, q);
+__device__ __forceinline__ uint32_t mod_sub(uint32_t a, uint32_t b, uint32_t q) {  // a, b < q
+  const uint32_t d = a - b;
+  return __viaddmin_u32(d, q, d);
 }
 // Shoup: a * w mod q for a constant w with wsh = floor(w * 2^32 / q); any a < 2^32.
 __device__ __forceinline__ uint32_t shoup_lazy(uint32_t a, uint32_t w, uint32_t wsh, uint32_t q) {

@@ -135,10 +135,11 @@ int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
       const uint32_t a = (uint32_t)pw[bitrev(i, logn)], b = (uint32_t)ipw[bitrev(i, logn)];
       h_psi[(size_t)m * n + i] = a;
       h_ipsi[(size_t)m * n + i] = b;
-      tab[(size_t)(0 * k + m) * n + i] = a;
-      tab[(size_t)(1 * k + m) * n + i] = shoup_of(a, (uint32_t)qq);
-      tab[(size_t)(2 * k + m) * n + i] = b;
-      tab[(size_t)(3 * k + m) * n + i] = shoup_of(b, (uint32_t)qq);
+      // interleaved (w, floor(w 2^32 / q)) pairs: psi2[k][n], then ipsi2[k][n]
+      tab[2 * ((size_t)m * n + i)] = a;
+      tab[2 * ((size_t)m * n + i) + 1] = shoup_of(a, (uint32_t)qq);
+      tab[2 * ((size_t)(k + m) * n + i)] = b;
+      tab[2 * ((size_t)(k + m) * n + i) + 1] = shoup_of(b, (uint32_t)qq);
     }
     args.q[m] = (uint32_t)qq;
     args.ninv[m] = (uint32_t)invmod(n, qq);
@@ -148,14 +149,13 @@ int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
   }
   args.n = n;
   args.logn = logn;
+  args.pp_fwd = args.pp_inv = 1;
   args.k = k;
   CUFE_CUDA(cudaSetDevice(device));
   CUFE_CUDA(cudaMalloc(&d_tab, tab.size() * 4));
   CUFE_CUDA(cudaMemcpy(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice));
-  args.psi = d_tab;
-  args.psi_sh = d_tab + (size_t)k * n;
-  args.ipsi = d_tab + 2 * (size_t)k * n;
-  args.ipsi_sh = d_tab + 3 * (size_t)k * n;
+  args.psi2 = reinterpret_cast<const uint2 *>(d_tab);
+  args.ipsi2 = reinterpret_cast<const uint2 *>(d_tab) + (size_t)k * n;
   return CUFE_OK;
 }
 
@@ -190,61 +190,189 @@ __device__ __forceinline__ void store16(uint32_t *p, const uint32_t (&a)[16]) {
   for (int i = 0; i < 4; ++i) v[i] = make_uint4(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]);
 }
 
-// MODE 0 forward, 1 forward + Shoup companions into sh, 2 inverse
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(512) k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long nres,
+// MODE 0 forward, 1 forward + Shoup companions into sh, 2 inverse.  data holds `rows`
+// polynomials of k residues ([row][k][n]); a thread group transforms PP residues of one
+// modulus m, rows PP*t .. PP*t+PP-1, sharing twiddles and shared-memory addresses.
+template <int LOGN, int MODE, int PP>
+__global__ void __launch_bounds__(512) k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows,
                                              RingArgs ra) {
   using P = NttPlan<LOGN>;
   extern __shared__ uint32_t smem_u32[];
-  const int th = threadIdx.x;
-  const long long r = (long long)blockIdx.x * blockDim.y + threadIdx.y;
-  const bool act = r < nres;
-  const long long rr = act ? r : nres - 1;
-  const int m = (int)(rr % ra.k);
+  const int th = threadIdx.x, k = ra.k;
+  const long long groups = (rows + PP - 1) / PP * k;
+  const long long gi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const long long gg = gi < groups ? gi : groups - 1;
+  const int m = (int)(gg % k);
+  const long long row0 = gg / k * PP;
   const uint32_t q = ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
-  uint32_t *d = data + rr * P::N;
-  uint32_t a[16];
+  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::N;
+  long long res[PP];
+  bool live[PP];
+#pragma unroll
+  for (int p = 0; p < PP; ++p) {
+    live[p] = gi < groups && row0 + p < rows;
+    res[p] = (live[p] ? row0 + p : row0) * k + m;  // a dead slot recomputes row0, stores nothing
+  }
+  uint32_t a[PP][16];
   if (MODE != 2) {
 #pragma unroll
-    for (int e = 0; e < 16; ++e) a[e] = d[P::template idx<0>(th, e)];
-    ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi + (size_t)m * P::N, ra.psi_sh + (size_t)m * P::N);
-    if (act) {
-      store16(d + th * 16, a);
+    for (int p = 0; p < PP; ++p) {
+      const uint32_t *d = data + res[p] * P::N;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) a[p][e] = d[P::template idx<0>(th, e)];
+    }
+    ntt_fwd_core<LOGN, PP>(a, sm, th, q, ra.psi2 + (size_t)m * P::N);
+#pragma unroll
+    for (int p = 0; p < PP; ++p) {
+      if (!live[p]) continue;
+      store16(data + res[p] * P::N + th * 16, a[p]);
       if (MODE == 1) {
         uint32_t b[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) b[e] = (uint32_t)(((uint64_t)a[e] << 32) / q);
-        store16(sh + rr * P::N + th * 16, b);
+        for (int e = 0; e < 16; ++e) b[e] = (uint32_t)(((uint64_t)a[p][e] << 32) / q);
+        store16(sh + res[p] * P::N + th * 16, b);
       }
     }
   } else {
-    load16(d + th * 16, a);
-    ntt_inv_core<LOGN>(a, sm, th, q, ra.ipsi + (size_t)m * P::N, ra.ipsi_sh + (size_t)m * P::N, ra.ninv[m],
-                       ra.ninv_sh[m], ra.w1n[m], ra.w1n_sh[m]);
-    if (act) {
 #pragma unroll
-      for (int e = 0; e < 16; ++e) d[P::template idx<0>(th, e)] = a[e];
+    for (int p = 0; p < PP; ++p) load16(data + res[p] * P::N + th * 16, a[p]);
+    ntt_inv_core<LOGN, PP>(a, sm, th, q, ra.ipsi2 + (size_t)m * P::N, ra.ninv[m], ra.ninv_sh[m], ra.w1n[m],
+                           ra.w1n_sh[m]);
+#pragma unroll
+    for (int p = 0; p < PP; ++p) {
+      if (!live[p]) continue;
+      uint32_t *d = data + res[p] * P::N;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) d[P::template idx<0>(th, e)] = a[p][e];
     }
   }
 }
 
+template <int LOGN, int MODE, int PP>
+int launch_ntt_pp(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long rows, cudaStream_t s) {
+  using P = NttPlan<LOGN>;
+  constexpr int G = ppc<LOGN>();
+  const size_t smem = (size_t)G * PP * P::N * 4;
+  static bool attr = false;
+  if (!attr) {
+    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    attr = true;
+  }
+  const long long groups = (rows + PP - 1) / PP * ra.k;
+  const long long grid = (groups + G - 1) / G;
+  if (grid <= 0) return CUFE_OK;
+  ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
+  k_ntt<LOGN, MODE, PP><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+// Persistent form: each thread group walks residues r, r + stride, ... and issues the global
+// loads of its next residue into registers before transforming the current one, so every
+// CTA keeps a residue's worth of loads in flight while it computes.  One residue per thread
+// group; the trip count is uniform per CTA (the exchanges synchronise the CTA).
 template <int LOGN, int MODE>
-int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
+__global__ void __maxnreg__(80) k_ntt_stream(uint32_t *__restrict__ data, uint32_t *__restrict__ sh,
+                                                    long long nres, RingArgs ra) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x;
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  const long long stride = (long long)gridDim.x * blockDim.y;
+  const long long cta0 = (long long)blockIdx.x * blockDim.y;
+  const long long iters = cta0 < nres ? (nres - cta0 + stride - 1) / stride : 0;
+  const long long r0 = cta0 + threadIdx.y;
+  uint32_t nx[16];
+  {
+    const uint32_t *d = data + (r0 < nres ? r0 : nres - 1) * P::N;
+    if (MODE != 2) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) nx[e] = d[P::template idx<0>(th, e)];
+    } else {
+      load16(d + th * 16, nx);
+    }
+  }
+  for (long long it = 0; it < iters; ++it) {
+    const long long cur = r0 + it * stride;
+    const bool act = cur < nres;
+    const long long cc = act ? cur : nres - 1;
+    uint32_t a[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) a[e] = nx[e];
+    if (it + 1 < iters) {
+      const long long nxt = cur + stride;
+      const uint32_t *d = data + (nxt < nres ? nxt : nres - 1) * P::N;
+      if (MODE != 2) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) nx[e] = d[P::template idx<0>(th, e)];
+      } else {
+        load16(d + th * 16, nx);
+      }
+    }
+    const int m = (int)(cc % ra.k);
+    const uint32_t q = ra.q[m];
+    uint32_t *d = data + cc * P::N;
+    if (MODE != 2) {
+      ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi2 + (size_t)m * P::N);
+      if (act) {
+        store16(d + th * 16, a);
+        if (MODE == 1) {
+          uint32_t b[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) b[e] = (uint32_t)(((uint64_t)a[e] << 32) / q);
+          store16(sh + cc * P::N + th * 16, b);
+        }
+      }
+    } else {
+      ntt_inv_core<LOGN>(a, sm, th, q, ra.ipsi2 + (size_t)m * P::N, ra.ninv[m], ra.ninv_sh[m], ra.w1n[m],
+                         ra.w1n_sh[m]);
+      if (act) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) d[P::template idx<0>(th, e)] = a[e];
+      }
+    }
+    __syncthreads();  // the next iteration's first exchange reuses sm
+  }
+}
+
+inline int device_sms() {
+  static int sms[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!sms[dev] && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    sms[dev] = 148;
+  return sms[dev];
+}
+
+template <int LOGN, int MODE>
+int launch_ntt_stream(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
   using P = NttPlan<LOGN>;
   constexpr int G = ppc<LOGN>();
   const size_t smem = (size_t)G * P::N * 4;
-  static bool attr = false;
-  if (!attr) {
-    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-    attr = true;
+  static int occ = 0;
+  if (!occ) {
+    CUFE_CUDA(cudaFuncSetAttribute(k_ntt_stream<LOGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CUFE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ntt_stream<LOGN, MODE>, P::T * G, smem));
+    if (occ < 1) occ = 1;
   }
-  const long long grid = (nres + G - 1) / G;
+  const long long need = (nres + G - 1) / G;
+  const long long grid = std::min(need, (long long)device_sms() * occ);
   if (grid <= 0) return CUFE_OK;
   ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
-  k_ntt<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
+  k_ntt_stream<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
+}
+
+// residues per thread group: the ring's tuned choice for this direction, else 1
+template <int LOGN, int MODE>
+int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
+  if (nres % ra.k) return CUFE_ERR_INVALID;
+  const long long rows = nres / ra.k;
+  const int pp = MODE == 2 ? ra.pp_inv : ra.pp_fwd;
+  if (pp == 3) return launch_ntt_stream<LOGN, MODE>(ra, data, sh, nres, s);
+  if (pp == 2 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2>(ra, data, sh, rows, s);
+  return launch_ntt_pp<LOGN, MODE, 1>(ra, data, sh, rows, s);
 }
 
 template <int MODE>
@@ -299,7 +427,7 @@ __global__ void __launch_bounds__(512) k_setup_mpk(const uint32_t *__restrict__ 
   uint32_t a[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) a[e] = msk[rr * P::N + P::template idx<0>(th, e)];
-  ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi + (size_t)m * P::N, ra.psi_sh + (size_t)m * P::N);
+  ntt_fwd_core<LOGN>(a, sm, th, q, ra.psi2 + (size_t)m * P::N);
   uint32_t w[16], wsh[16], ev[16];
   load16(ahat + (size_t)m * P::N + th * 16, w);
   load16(ahat_sh + (size_t)m * P::N + th * 16, wsh);
@@ -336,7 +464,7 @@ __global__ void __launch_bounds__(512)
   load16(rhat_sh + b * rhat_stride + (size_t)m * P::N + th * 16, wsh);
 #pragma unroll
   for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
-  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi + (size_t)m * P::N, sa.ra.ipsi_sh + (size_t)m * P::N, sa.ra.ninv[m],
+  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi2 + (size_t)m * P::N, sa.ra.ninv[m],
                      sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
   const uint32_t *f;
   uint32_t msg = 0;
@@ -454,7 +582,7 @@ __global__ void __launch_bounds__(512)
   load16(skhat_sh + ((size_t)key * 3 + m) * P::N + th * 16, wsh);
 #pragma unroll
   for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
-  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi + (size_t)m * P::N, sa.ra.ipsi_sh + (size_t)m * P::N, sa.ra.ninv[m],
+  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi2 + (size_t)m * P::N, sa.ra.ninv[m],
                      sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
   if (act) {
     const uint32_t *pp = part + (size_t)ww * nsplit * P::N;
@@ -578,6 +706,53 @@ int ntt_launch(const RingArgs &ra, uint32_t *data, long long nres, bool inverse,
 }
 int ntt_fwd_shoup_launch(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
   return launch_ntt<1>(ra, data, sh, nres, s);
+}
+
+int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s) {
+  const size_t poly_bytes = (size_t)r.k * r.n * 4;
+  npoly = std::max(2LL, std::min(npoly, (long long)((1ull << 30) / poly_bytes)));
+  uint32_t *buf = nullptr;
+  CUFE_CUDA(cudaMalloc(&buf, (size_t)npoly * poly_bytes));
+  // zero residues: the kernels' instruction stream does not depend on the values
+  cudaError_t err = cudaMemsetAsync(buf, 0, (size_t)npoly * poly_bytes, s);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  constexpr int NV = 3;
+  float t[2 * NV] = {0, 0, 0, 0, 0, 0};
+  int rc = CUFE_OK;
+  if (err == cudaSuccess) err = cudaEventCreate(&e0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e1);
+  const RingArgs saved = r.args;
+  for (int i = 0; i < 2 * NV && err == cudaSuccess && rc == CUFE_OK; ++i) {
+    const bool inv = i >= NV;
+    r.args.pp_fwd = r.args.pp_inv = 1 + i % NV;
+    const long long nres = npoly * r.k;
+    rc = ntt_launch(r.args, buf, nres, inv, s);  // warm-up
+    if (rc) break;
+    if ((err = cudaEventRecord(e0, s)) != cudaSuccess) break;
+    for (int rep = 0; rep < 3 && rc == CUFE_OK; ++rep) rc = ntt_launch(r.args, buf, nres, inv, s);
+    if (rc || (err = cudaEventRecord(e1, s)) != cudaSuccess || (err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+    if ((err = cudaEventElapsedTime(&t[i], e0, e1)) != cudaSuccess) break;
+    t[i] /= 3.0f;
+  }
+  r.args = saved;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (rc) return rc;
+  if (err != cudaSuccess) {
+    set_last_error(std::string("ring_tune: ") + cudaGetErrorString(err));
+    return CUFE_ERR_CUDA;
+  }
+  int bf = 0, bi = NV;
+  for (int v = 1; v < NV; ++v) {
+    if (t[v] < t[bf]) bf = v;
+    if (t[NV + v] < t[bi]) bi = NV + v;
+  }
+  r.args.pp_fwd = 1 + bf;
+  r.args.pp_inv = 1 + bi - NV;
+  if (ms)
+    for (int i = 0; i < 2 * NV; ++i) ms[i] = t[i];
+  return CUFE_OK;
 }
 
 // ================================================================== context

@@ -41,56 +41,94 @@ struct NttPlan {
   __device__ __forceinline__ static int swz(int j) { return j ^ ((j >> 4) & 31); }
 };
 
-template <int LOGN, int FROM, int TO>
-__device__ __forceinline__ void ntt_exchange(uint32_t (&a)[16], uint32_t *sm, int th) {
+// P residue polynomials per thread group (same modulus, shared twiddles and addresses):
+// polynomial p uses registers a[p][] and shared words sm[p * N ...]
+template <int LOGN, int FROM, int TO, int P_>
+__device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][16], uint32_t *sm, int th) {
   using P = NttPlan<LOGN>;
 #pragma unroll
-  for (int e = 0; e < 16; ++e) sm[P::swz(P::template idx<FROM>(th, e))] = a[e];
+  for (int e = 0; e < 16; ++e) {
+    const int j = P::swz(P::template idx<FROM>(th, e));
+#pragma unroll
+    for (int p = 0; p < P_; ++p) sm[p * P::N + j] = a[p][e];
+  }
   __syncthreads();
 #pragma unroll
-  for (int e = 0; e < 16; ++e) a[e] = sm[P::swz(P::template idx<TO>(th, e))];
+  for (int e = 0; e < 16; ++e) {
+    const int j = P::swz(P::template idx<TO>(th, e));
+#pragma unroll
+    for (int p = 0; p < P_; ++p) a[p][e] = sm[p * P::N + j];
+  }
 }
 
 struct InvScale {
   uint32_t ninv, ninv_sh, w1n, w1n_sh;
 };
 
+// twiddles (w, w_shoup) tw[ti0 .. ti0+NG-1]: pairs of entries per 16-byte load when NG >= 2
+// (ti0 is then even, so the load is aligned)
+template <int NG>
+__device__ __forceinline__ void load_twiddles(const uint2 *__restrict__ tw, int ti0, uint32_t (&w)[NG],
+                                              uint32_t (&wsh)[NG]) {
+  if constexpr (NG == 1) {
+    const uint2 t = __ldg(tw + ti0);
+    w[0] = t.x;
+    wsh[0] = t.y;
+  } else {
+    const uint4 *t4 = reinterpret_cast<const uint4 *>(tw + ti0);
+#pragma unroll
+    for (int g = 0; g < NG / 2; ++g) {
+      const uint4 t = __ldg(t4 + g);
+      w[2 * g] = t.x;
+      wsh[2 * g] = t.y;
+      w[2 * g + 1] = t.z;
+      wsh[2 * g + 1] = t.w;
+    }
+  }
+}
+
 // stage LS of pass PASS (CT stage s = first_stage(PASS) + LS; the inverse runs the same
 // butterfly positions with Gentleman-Sande butterflies and psi^-1 twiddles)
-template <int LOGN, int PASS, int LS, bool INV>
-__device__ __forceinline__ void ntt_stage(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *__restrict__ tw,
-                                          const uint32_t *__restrict__ twsh, const InvScale &sc) {
+template <int LOGN, int PASS, int LS, bool INV, int P_>
+__device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *__restrict__ tw,
+                                          const InvScale &sc) {
   using P = NttPlan<LOGN>;
   constexpr int rb = P::radix_bits(PASS), s0 = P::first_stage(PASS), plo = LOGN - s0 - rb;
   constexpr int s = s0 + LS, half = 1 << (rb - 1 - LS), nv = 16 >> rb, ng = 1 << LS;
 #pragma unroll
   for (int v = 0; v < nv; ++v) {
     const int H = (v * P::T + th) >> plo;
+    if constexpr (INV && s == 0) {
 #pragma unroll
-    for (int g = 0; g < ng; ++g) {
-      if constexpr (INV && s == 0) {
+      for (int b = 0; b < half; ++b) {
+        const int e1 = (v << rb) + b, e2 = e1 + half;
 #pragma unroll
-        for (int b = 0; b < half; ++b) {
-          const int e1 = (v << rb) + g * 2 * half + b, e2 = e1 + half;
-          const uint32_t U = a[e1], V = a[e2];
-          a[e1] = shoup_mul(U + V, sc.ninv, sc.ninv_sh, q);
-          a[e2] = shoup_mul(U - V + q, sc.w1n, sc.w1n_sh, q);
+        for (int p = 0; p < P_; ++p) {
+          const uint32_t U = a[p][e1], V = a[p][e2];
+          a[p][e1] = shoup_mul(U + V, sc.ninv, sc.ninv_sh, q);
+          a[p][e2] = shoup_mul(U - V + q, sc.w1n, sc.w1n_sh, q);
         }
-      } else {
-        const int ti = (1 << s) + ((H << LS) | g);
-        const uint32_t w = __ldg(tw + ti), wsh = __ldg(twsh + ti);
+      }
+    } else {
+      uint32_t w[ng], wsh[ng];
+      load_twiddles<ng>(tw, (1 << s) + (H << LS), w, wsh);
+#pragma unroll
+      for (int g = 0; g < ng; ++g) {
 #pragma unroll
         for (int b = 0; b < half; ++b) {
           const int e1 = (v << rb) + g * 2 * half + b, e2 = e1 + half;
-          if constexpr (!INV) {
-            const uint32_t V = shoup_mul(a[e2], w, wsh, q);
-            const uint32_t U = a[e1];
-            a[e1] = mod_add(U, V, q);
-            a[e2] = mod_sub(U, V, q);
-          } else {
-            const uint32_t U = a[e1], V = a[e2];
-            a[e1] = mod_add(U, V, q);
-            a[e2] = shoup_mul(U - V + q, w, wsh, q);
+#pragma unroll
+          for (int p = 0; p < P_; ++p) {
+            if constexpr (!INV) {
+              const uint32_t V = shoup_mul(a[p][e2], w[g], wsh[g], q);
+              const uint32_t U = a[p][e1];
+              a[p][e1] = mod_add(U, V, q);
+              a[p][e2] = mod_sub(U, V, q);
+            } else {
+              const uint32_t U = a[p][e1], V = a[p][e2];
+              a[p][e1] = mod_add(U, V, q);
+              a[p][e2] = shoup_mul(U - V + q, w[g], wsh[g], q);
+            }
           }
         }
       }
@@ -98,50 +136,58 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[16], int th, uint32_t q,
   }
 }
 
-template <int LOGN, int PASS, int LS>
-__device__ __forceinline__ void ntt_fwd_stages(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *tw,
-                                               const uint32_t *twsh) {
-  ntt_stage<LOGN, PASS, LS, false>(a, th, q, tw, twsh, InvScale{});
-  if constexpr (LS + 1 < NttPlan<LOGN>::radix_bits(PASS)) ntt_fwd_stages<LOGN, PASS, LS + 1>(a, th, q, tw, twsh);
+template <int LOGN, int PASS, int LS, int P_>
+__device__ __forceinline__ void ntt_fwd_stages(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *tw) {
+  ntt_stage<LOGN, PASS, LS, false, P_>(a, th, q, tw, InvScale{});
+  if constexpr (LS + 1 < NttPlan<LOGN>::radix_bits(PASS)) ntt_fwd_stages<LOGN, PASS, LS + 1, P_>(a, th, q, tw);
 }
-template <int LOGN, int PASS>
-__device__ __forceinline__ void ntt_fwd_passes(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q, const uint32_t *tw,
-                                               const uint32_t *twsh) {
-  if constexpr (PASS > 0) ntt_exchange<LOGN, PASS - 1, PASS>(a, sm, th);
-  ntt_fwd_stages<LOGN, PASS, 0>(a, th, q, tw, twsh);
-  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_fwd_passes<LOGN, PASS + 1>(a, sm, th, q, tw, twsh);
+template <int LOGN, int PASS, int P_>
+__device__ __forceinline__ void ntt_fwd_passes(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+                                               const uint2 *tw) {
+  if constexpr (PASS > 0) ntt_exchange<LOGN, PASS - 1, PASS, P_>(a, sm, th);
+  ntt_fwd_stages<LOGN, PASS, 0, P_>(a, th, q, tw);
+  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_fwd_passes<LOGN, PASS + 1, P_>(a, sm, th, q, tw);
 }
-template <int LOGN, int PASS, int LS>
-__device__ __forceinline__ void ntt_inv_stages(uint32_t (&a)[16], int th, uint32_t q, const uint32_t *tw,
-                                               const uint32_t *twsh, const InvScale &sc) {
-  ntt_stage<LOGN, PASS, LS, true>(a, th, q, tw, twsh, sc);
-  if constexpr (LS > 0) ntt_inv_stages<LOGN, PASS, LS - 1>(a, th, q, tw, twsh, sc);
+template <int LOGN, int PASS, int LS, int P_>
+__device__ __forceinline__ void ntt_inv_stages(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *tw,
+                                               const InvScale &sc) {
+  ntt_stage<LOGN, PASS, LS, true, P_>(a, th, q, tw, sc);
+  if constexpr (LS > 0) ntt_inv_stages<LOGN, PASS, LS - 1, P_>(a, th, q, tw, sc);
 }
-template <int LOGN, int PASS>
-__device__ __forceinline__ void ntt_inv_passes(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q, const uint32_t *tw,
-                                               const uint32_t *twsh, const InvScale &sc) {
-  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_exchange<LOGN, PASS + 1, PASS>(a, sm, th);
-  ntt_inv_stages<LOGN, PASS, NttPlan<LOGN>::radix_bits(PASS) - 1>(a, th, q, tw, twsh, sc);
-  if constexpr (PASS > 0) ntt_inv_passes<LOGN, PASS - 1>(a, sm, th, q, tw, twsh, sc);
+template <int LOGN, int PASS, int P_>
+__device__ __forceinline__ void ntt_inv_passes(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+                                               const uint2 *tw, const InvScale &sc) {
+  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_exchange<LOGN, PASS + 1, PASS, P_>(a, sm, th);
+  ntt_inv_stages<LOGN, PASS, NttPlan<LOGN>::radix_bits(PASS) - 1, P_>(a, th, q, tw, sc);
+  if constexpr (PASS > 0) ntt_inv_passes<LOGN, PASS - 1, P_>(a, sm, th, q, tw, sc);
 }
 
-// Registers a[] hold the pass-0 layout on entry and the last-pass layout (16 consecutive
-// coefficients th*16 .. th*16+15) on exit.  sm: this polynomial's SMEM_WORDS scratch.
+// Registers a[p][] hold the pass-0 layout on entry and the last-pass layout (16 consecutive
+// coefficients th*16 .. th*16+15) on exit.  sm: P_ x SMEM_WORDS scratch for this group.
+template <int LOGN, int P_>
+__device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+                                             const uint2 *__restrict__ psi2) {
+  ntt_fwd_passes<LOGN, 0, P_>(a, sm, th, q, psi2);
+}
 template <int LOGN>
 __device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,
-                                             const uint32_t *__restrict__ psi,
-                                             const uint32_t *__restrict__ psh) {
-  ntt_fwd_passes<LOGN, 0>(a, sm, th, q, psi, psh);
+                                             const uint2 *__restrict__ psi2) {
+  ntt_fwd_core<LOGN, 1>(reinterpret_cast<uint32_t(&)[1][16]>(a), sm, th, q, psi2);
 }
 
 // Registers hold the last-pass layout (16 consecutive coefficients) on entry and the
 // pass-0 layout on exit.  Inputs must be canonical residues.
+template <int LOGN, int P_>
+__device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+                                             const uint2 *__restrict__ ipsi2, uint32_t ninv, uint32_t ninv_sh,
+                                             uint32_t w1n, uint32_t w1n_sh) {
+  ntt_inv_passes<LOGN, NttPlan<LOGN>::NP - 1, P_>(a, sm, th, q, ipsi2, InvScale{ninv, ninv_sh, w1n, w1n_sh});
+}
 template <int LOGN>
 __device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,
-                                             const uint32_t *__restrict__ ipsi,
-                                             const uint32_t *__restrict__ ipsh, uint32_t ninv,
-                                             uint32_t ninv_sh, uint32_t w1n, uint32_t w1n_sh) {
-  ntt_inv_passes<LOGN, NttPlan<LOGN>::NP - 1>(a, sm, th, q, ipsi, ipsh, InvScale{ninv, ninv_sh, w1n, w1n_sh});
+                                             const uint2 *__restrict__ ipsi2, uint32_t ninv, uint32_t ninv_sh,
+                                             uint32_t w1n, uint32_t w1n_sh) {
+  ntt_inv_core<LOGN, 1>(reinterpret_cast<uint32_t(&)[1][16]>(a), sm, th, q, ipsi2, ninv, ninv_sh, w1n, w1n_sh);
 }
 
 }  // namespace cufe

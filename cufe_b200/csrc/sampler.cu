@@ -104,25 +104,42 @@ __host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : w - 12; 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
 constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed with p < 1e-7
 
+// stream of a flattened index: the s with off[s] <= g < off[s+1] (off non-decreasing, size S+1)
+template <typename T>
+__device__ __forceinline__ uint32_t seg_find(const T *__restrict__ off, uint32_t nseg, uint64_t g) {
+  uint32_t lo = 0, hi = nseg;  // off[lo] <= g < off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((uint64_t)__ldg(off + mid) <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)
-    k_cand_cpu(const uint32_t *__restrict__ rkeys, uint32_t nstreams, uint32_t refills, double kinv,
-               int64_t *__restrict__ cand, uint8_t *__restrict__ amask, uint32_t *__restrict__ status) {
+    k_cand_cpu(const uint32_t *__restrict__ rkeys, SegDev sg, double kinv, int64_t *__restrict__ cand,
+               uint8_t *__restrict__ amask, uint32_t *__restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
   aes_fill_tables(smem);
   __syncthreads();
   const AesCtx c{smem, (threadIdx.x & 31u) * 4u};
-  const uint32_t total = nstreams * refills;
+  // the host keeps the flattened refill count below 2^32 - 2^24 (no wrap of g)
+  const uint32_t total = (uint32_t)__ldg(sg.roff + sg.nstreams);
   uint32_t rk[60];
-  uint32_t cur = 0xffffffffu;
+  uint32_t st = 0;
+  uint32_t lo = 1, hi = 0;  // refill range of stream st (empty: forces the first lookup)
+  const uint32_t *rkg = rkeys;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
-    const uint32_t st = g / refills, t = g - st * refills;
-    const uint32_t *rkg = rkeys + (size_t)st * 60;
-    if (st != cur) {
+    if (g < lo || g >= hi) {
+      st = seg_find(sg.roff, sg.nstreams, g);
+      lo = (uint32_t)__ldg(sg.roff + st);
+      hi = (uint32_t)__ldg(sg.roff + st + 1);
+      rkg = rkeys + (size_t)st * 60;
 #pragma unroll
       for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
-      cur = st;
     }
+    const uint32_t t = g - lo;
     const uint32_t cb = t * 24u;
     // 1. the keystream blocks, one AES body (keeps the loop inside the instruction cache)
     uint4 buf4[kRefillBlocks];
@@ -182,18 +199,20 @@ __global__ void __launch_bounds__(kCandThreads, 1)
 
 constexpr int kScanTile = 4096;  // refills per scan tile (512 threads x 8)
 
-// per-tile exclusive scan of accept counts; E_local[t], tile sums
-__global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ amask, uint32_t refills,
-                                                    uint32_t tiles, uint32_t *__restrict__ elocal,
-                                                    uint32_t *__restrict__ tile_sum) {
+// per-tile exclusive scan of accept counts: elocal[g] (within the tile), tile_sum[tile];
+// one CTA per tile of the flattened tile space
+__global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ amask, SegDev sg,
+                                                    uint32_t *__restrict__ elocal, uint32_t *__restrict__ tile_sum) {
   __shared__ uint32_t wsum[16];
-  const uint32_t st = blockIdx.y, tile = blockIdx.x;
-  const uint32_t base = tile * kScanTile + threadIdx.x * 8;
+  const uint32_t T = blockIdx.x;
+  const uint32_t st = seg_find(sg.toff, sg.nstreams, T);
+  const uint64_t r0 = __ldg(sg.roff + st), R = __ldg(sg.roff + st + 1) - r0;
+  const uint64_t base = (uint64_t)(T - __ldg(sg.toff + st)) * kScanTile + threadIdx.x * 8;
   uint32_t cnt[8], tot = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const uint32_t t = base + i;
-    cnt[i] = t < refills ? __popc(amask[(size_t)st * refills + t]) : 0u;
+    const uint64_t t = base + i;
+    cnt[i] = t < R ? __popc(amask[r0 + t]) : 0u;
     tot += cnt[i];
   }
   // block exclusive scan of per-thread totals
@@ -214,29 +233,30 @@ __global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ 
       if (lane >= o) si += v;
     }
     if (lane < 16) wsum[lane] = si - s;
-    if (lane == 15) tile_sum[(size_t)st * tiles + tile] = si;
+    if (lane == 15) tile_sum[T] = si;
   }
   __syncthreads();
   uint32_t run = wsum[wid] + inc - tot;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const uint32_t t = base + i;
-    if (t < refills) elocal[(size_t)st * refills + t] = run;
+    const uint64_t t = base + i;
+    if (t < R) elocal[r0 + t] = run;
     run += cnt[i];
   }
 }
 
-// exclusive scan of tile sums per stream (one block per stream)
-__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *__restrict__ tile_sum, uint32_t tiles) {
+// exclusive scan of the tile sums of each stream (one block per stream)
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *__restrict__ tile_sum, SegDev sg) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t carry;
   const uint32_t st = blockIdx.x;
+  const uint32_t t0 = __ldg(sg.toff + st), tiles = __ldg(sg.toff + st + 1) - t0;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   for (uint32_t b0 = 0; b0 < tiles; b0 += 1024) {
     const uint32_t i = b0 + threadIdx.x;
-    const uint32_t v = i < tiles ? tile_sum[(size_t)st * tiles + i] : 0u;
+    const uint32_t v = i < tiles ? tile_sum[t0 + i] : 0u;
     uint32_t inc = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -256,37 +276,50 @@ __global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *__restrict__ tile_
     }
     __syncthreads();
     const uint32_t excl = carry + wsum[wid] + inc - v;
-    if (i < tiles) tile_sum[(size_t)st * tiles + i] = excl;
+    if (i < tiles) tile_sum[t0 + i] = excl;
     __syncthreads();
     if (threadIdx.x == 1023) carry = excl + v;
     __syncthreads();
   }
 }
 
-__device__ __forceinline__ uint32_t prefix_at(const uint32_t *elocal, const uint32_t *tile_off,
-                                              const uint8_t *amask, uint32_t refills, uint32_t tiles,
-                                              uint32_t st, uint32_t t) {
-  // exclusive prefix E(t) for t in [0, refills]
-  if (t < refills) return elocal[(size_t)st * refills + t] + tile_off[(size_t)st * tiles + t / kScanTile];
-  const uint32_t l = refills - 1;
-  return elocal[(size_t)st * refills + l] + tile_off[(size_t)st * tiles + l / kScanTile] +
-         __popc(amask[(size_t)st * refills + l]);
+// exclusive prefix E(t) of stream st's accept counts, t in [0, R]
+struct SegView {
+  uint64_t r0;
+  uint32_t R, t0;
+};
+__device__ __forceinline__ SegView seg_view(const SegDev &sg, uint32_t st) {
+  SegView v;
+  v.r0 = __ldg(sg.roff + st);
+  v.R = (uint32_t)(__ldg(sg.roff + st + 1) - v.r0);
+  v.t0 = __ldg(sg.toff + st);
+  return v;
+}
+__device__ __forceinline__ uint32_t prefix_at(const uint32_t *elocal, const uint32_t *tile_off, const uint8_t *amask,
+                                              const SegView &v, uint32_t t) {
+  if (t < v.R) return elocal[v.r0 + t] + tile_off[v.t0 + t / kScanTile];
+  const uint32_t l = v.R - 1;
+  return elocal[v.r0 + l] + tile_off[v.t0 + l / kScanTile] + __popc(amask[v.r0 + l]);
 }
 
 // one warp per stream: call c starts at a fresh refill a_c; it ends at the first refill e
-// whose inclusive prefix reaches E(a_c) + n; a_{c+1} = e + 1.
+// whose inclusive prefix reaches E(a_c) + n; a_{c+1} = e + 1.  call_start of stream st:
+// coff[st] + st .. coff[st+1] + st (calls + 1 entries; the last is the end of the last call).
 __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__restrict__ tile_off,
-                       const uint8_t *__restrict__ amask, uint32_t refills, uint32_t tiles, uint32_t calls,
-                       uint32_t n, uint32_t guess, uint32_t nstreams, uint32_t *__restrict__ call_start,
-                       uint32_t *__restrict__ status) {
+                       const uint8_t *__restrict__ amask, SegDev sg, float mean_accept,
+                       uint32_t *__restrict__ call_start, uint32_t *__restrict__ status) {
   const uint32_t st = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (st >= nstreams) return;  // whole warps only
+  if (st >= sg.nstreams) return;  // whole warps only
+  const SegView v = seg_view(sg, st);
+  const uint32_t n = __ldg(sg.n + st), calls = __ldg(sg.calls + st);
+  const uint32_t guess = (uint32_t)((float)n / mean_accept);
+  uint32_t *cs = call_start + __ldg(sg.coff + st) + st;
   uint32_t a = 0;
-  bool bad = false;
+  bool bad = v.R == 0;
   uint32_t c = 0;
   for (; c < calls && !bad; ++c) {
-    const uint32_t base = prefix_at(elocal, tile_off, amask, refills, tiles, st, a);
+    const uint32_t base = prefix_at(elocal, tile_off, amask, v, a);
     const uint32_t target = base + n;
     // smallest e >= a whose inclusive prefix reaches target (monotone in e), searched in
     // windows of 32 refills around the expected call length; `known` is a position already
@@ -300,14 +333,14 @@ __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__re
         break;
       }
       const uint32_t j = lo + lane;
-      const bool ok = (j < refills) && prefix_at(elocal, tile_off, amask, refills, tiles, st, j + 1) >= target;
+      const bool ok = (j < v.R) && prefix_at(elocal, tile_off, amask, v, j + 1) >= target;
       const uint32_t bal = __ballot_sync(0xffffffffu, ok);
       if (bal == 0) {
         if (known >= 0) {
           e = (uint32_t)known;
           break;
         }
-        if (lo + 32 >= refills) {
+        if (lo + 32 >= v.R) {
           bad = true;
           break;
         }
@@ -323,13 +356,12 @@ __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__re
       lo = lo > a + 32 ? lo - 32 : a;
     }
     if (bad) break;
-    if (lane == 0) call_start[(size_t)st * (calls + 1) + c] = a;
+    if (lane == 0) cs[c] = a;
     a = e + 1;
   }
   if (lane == 0) {
     if (bad) atomicOr(status, kStatusRefillsExhausted);
-    for (uint32_t r = bad ? c : calls; r <= calls; ++r)
-      call_start[(size_t)st * (calls + 1) + r] = bad ? refills : a;
+    for (uint32_t r = bad ? c : calls; r <= calls; ++r) cs[r] = bad ? v.R : a;
   }
 }
 
@@ -346,34 +378,56 @@ __device__ __forceinline__ uint32_t signed_residue(int64_t s, uint32_t q, uint64
   return r ? q - r : 0u;
 }
 
-// one CTA per (call, stream): accepted candidates of refills [a_c, a_{c+1}) in order
+// one CTA per call of the flattened call space: the accepted candidates of refills
+// [a_c, a_{c+1}) in order, as residues out[ooff[st] + c * 3n ...][3][n]
 __global__ void __launch_bounds__(256) k_scatter(const int64_t *__restrict__ cand, const uint8_t *__restrict__ amask,
                                                  const uint32_t *__restrict__ elocal,
                                                  const uint32_t *__restrict__ tile_off,
-                                                 const uint32_t *__restrict__ call_start, uint32_t refills,
-                                                 uint32_t tiles, uint32_t calls, uint32_t n, ModArgs m,
+                                                 const uint32_t *__restrict__ call_start, SegDev sg, ModArgs m,
                                                  uint32_t *__restrict__ out) {
-  const uint32_t c = blockIdx.x, st = blockIdx.y;
-  const uint32_t a = call_start[(size_t)st * (calls + 1) + c];
-  const uint32_t b = call_start[(size_t)st * (calls + 1) + c + 1];
-  if (a >= refills) return;
-  const uint32_t base = prefix_at(elocal, tile_off, amask, refills, tiles, st, a);
-  uint32_t *o = out + ((size_t)st * calls + c) * 3 * n;
-  for (uint32_t t = a + threadIdx.x; t < b && t < refills; t += blockDim.x) {
-    const uint32_t g = st * refills + t;
+  const uint32_t st = seg_find(sg.coff, sg.nstreams, blockIdx.x);
+  const uint64_t cs0 = __ldg(sg.coff + st);
+  const uint32_t c = (uint32_t)(blockIdx.x - cs0);
+  const SegView v = seg_view(sg, st);
+  const uint32_t n = __ldg(sg.n + st);
+  const uint32_t *cs = call_start + cs0 + st;
+  const uint32_t a = cs[c], b = cs[c + 1];
+  if (a >= v.R) return;
+  const uint32_t base = prefix_at(elocal, tile_off, amask, v, a);
+  uint32_t *o = out + __ldg(sg.ooff + st) + (size_t)c * 3 * n;
+  for (uint32_t t = a + threadIdx.x; t < b && t < v.R; t += blockDim.x) {
+    const uint64_t g = v.r0 + t;
     uint32_t msk = amask[g];
-    uint32_t pos = prefix_at(elocal, tile_off, amask, refills, tiles, st, t) - base;
-    const int64_t *cv = cand + (size_t)g * 8;
+    uint32_t pos = prefix_at(elocal, tile_off, amask, v, t) - base;
+    const int64_t *cv = cand + g * 8;
     while (msk) {
       const int i = __ffs(msk) - 1;
       msk &= msk - 1;
       if (pos < n) {
-        const int64_t s = cv[i];
+        const int64_t sv = cv[i];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) o[j * n + pos] = signed_residue(s, m.q[j], m.mu[j]);
+        for (int j = 0; j < 3; ++j) o[j * n + pos] = signed_residue(sv, m.q[j], m.mu[j]);
       }
       ++pos;
     }
+  }
+}
+
+// segment table of nstreams equal streams (calls x n each, refills R each, output stride
+// `ostride` words per stream)
+__global__ void k_seg_uniform(uint32_t nstreams, uint32_t calls, uint32_t n, uint32_t R, uint32_t tiles,
+                              uint64_t ostride, uint32_t *__restrict__ sn, uint32_t *__restrict__ scalls,
+                              uint64_t *__restrict__ roff, uint32_t *__restrict__ toff, uint64_t *__restrict__ coff,
+                              uint64_t *__restrict__ ooff) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nstreams) return;
+  roff[i] = (uint64_t)i * R;
+  toff[i] = i * tiles;
+  coff[i] = (uint64_t)i * calls;
+  if (i < nstreams) {
+    sn[i] = n;
+    scalls[i] = calls;
+    ooff[i] = (uint64_t)i * ostride;
   }
 }
 
@@ -601,19 +655,6 @@ int sampler_init_device() {
 // measurements (5.44, 4.39, 3.09 for S1, S2, S3; the truncations of Q5 reject more at large K)
 static double mean_accept(int sig) { return sig == 0 ? 5.35 : (sig == 1 ? 4.3 : 3.0); }
 
-size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, int sig) {
-  const uint32_t R = cpu_map_refills(calls, n, sig);
-  const uint32_t tiles = (R + kScanTile - 1) / kScanTile;
-  size_t b = 0;
-  auto add = [&](size_t x) { b += (x + 255) & ~(size_t)255; };
-  add((size_t)nstreams * R * 64);        // candidates
-  add((size_t)nstreams * R);             // masks
-  add((size_t)nstreams * R * 4);         // local prefix
-  add((size_t)nstreams * tiles * 4);     // tile sums
-  add((size_t)nstreams * (calls + 1) * 4);  // call starts
-  return b;
-}
-
 uint32_t cpu_map_refills(uint32_t calls, uint32_t n, int sig) {
   const double mu = mean_accept(sig);
   const double need = (double)calls * ((double)n / mu + 1.0);
@@ -621,71 +662,174 @@ uint32_t cpu_map_refills(uint32_t calls, uint32_t n, int sig) {
   return (R + 31) & ~31u;
 }
 
-int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
-                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+SegLayout seg_layout(uint32_t S) {
+  SegLayout L;
+  size_t o = 0;
+  L.n = o;
+  o += align256((size_t)S * 4);
+  L.calls = o;
+  o += align256((size_t)S * 4);
+  L.toff = o;
+  o += align256((size_t)(S + 1) * 4);
+  L.roff = o;
+  o += align256((size_t)(S + 1) * 8);
+  L.coff = o;
+  o += align256((size_t)(S + 1) * 8);
+  L.ooff = o;
+  o += align256((size_t)S * 8);
+  L.bytes = o;
+  return L;
+}
+
+SegDev seg_bind(void *base, uint32_t S) {
+  const SegLayout L = seg_layout(S);
+  uint8_t *b = static_cast<uint8_t *>(base);
+  SegDev d;
+  d.nstreams = S;
+  d.n = reinterpret_cast<const uint32_t *>(b + L.n);
+  d.calls = reinterpret_cast<const uint32_t *>(b + L.calls);
+  d.toff = reinterpret_cast<const uint32_t *>(b + L.toff);
+  d.roff = reinterpret_cast<const uint64_t *>(b + L.roff);
+  d.coff = reinterpret_cast<const uint64_t *>(b + L.coff);
+  d.ooff = reinterpret_cast<const uint64_t *>(b + L.ooff);
+  return d;
+}
+
+SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_t *n, const uint64_t *ooff,
+                       void *host_base) {
+  const SegLayout L = seg_layout(S);
+  uint8_t *b = static_cast<uint8_t *>(host_base);
+  uint32_t *hn = reinterpret_cast<uint32_t *>(b + L.n), *hc = reinterpret_cast<uint32_t *>(b + L.calls);
+  uint32_t *ht = reinterpret_cast<uint32_t *>(b + L.toff);
+  uint64_t *hr = reinterpret_cast<uint64_t *>(b + L.roff), *hco = reinterpret_cast<uint64_t *>(b + L.coff);
+  uint64_t *ho = reinterpret_cast<uint64_t *>(b + L.ooff);
+  SegSizes z{S, 0, 0, 0};
+  for (uint32_t i = 0; i < S; ++i) {
+    const uint32_t R = cpu_map_refills(calls[i], n[i], sig);
+    hn[i] = n[i];
+    hc[i] = calls[i];
+    ho[i] = ooff ? ooff[i] : 0;
+    hr[i] = z.refills;
+    ht[i] = z.tiles;
+    hco[i] = z.calls;
+    z.refills += R;
+    z.tiles += (R + kScanTile - 1) / kScanTile;
+    z.calls += calls[i];
+  }
+  hr[S] = z.refills;
+  ht[S] = z.tiles;
+  hco[S] = z.calls;
+  return z;
+}
+
+static SegSizes seg_uniform_sizes(uint32_t S, uint32_t calls, uint32_t n, int sig) {
   const uint32_t R = cpu_map_refills(calls, n, sig);
-  const uint32_t tiles = (R + kScanTile - 1) / kScanTile;
-  if ((uint64_t)nstreams * R >= (1ull << 32) - 1) return CUFE_ERR_INVALID;
-  uint8_t *p = static_cast<uint8_t *>(ws);
+  return SegSizes{S, (uint64_t)S * R, S * ((R + kScanTile - 1) / kScanTile), (uint64_t)S * calls};
+}
+
+size_t seg_scratch_bytes(const SegSizes &z) {
+  return align256(z.refills * 64) + align256(z.refills) + align256(z.refills * 4) + align256((size_t)z.tiles * 4) +
+         align256((z.calls + z.nstreams) * 4);
+}
+
+size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, int sig) {
+  return seg_layout(nstreams).bytes + seg_scratch_bytes(seg_uniform_sizes(nstreams, calls, n, sig));
+}
+
+int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint32_t *d_rkeys, uint32_t *d_out,
+                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
+  if (sig < 0 || sig > 2 || z.nstreams == 0 || z.tiles >= (1u << 31) || z.calls >= (1ull << 31) ||
+      z.refills >= (1ull << 32) - (1ull << 24))
+    return CUFE_ERR_INVALID;
+  uint8_t *p = static_cast<uint8_t *>(scratch);
   auto take = [&](size_t x) {
     uint8_t *r = p;
-    p += (x + 255) & ~(size_t)255;
+    p += align256(x);
     return r;
   };
-  int64_t *cand = reinterpret_cast<int64_t *>(take((size_t)nstreams * R * 64));
-  uint8_t *amask = take((size_t)nstreams * R);
-  uint32_t *elocal = reinterpret_cast<uint32_t *>(take((size_t)nstreams * R * 4));
-  uint32_t *tsum = reinterpret_cast<uint32_t *>(take((size_t)nstreams * tiles * 4));
-  uint32_t *cstart = reinterpret_cast<uint32_t *>(take((size_t)nstreams * (calls + 1) * 4));
+  int64_t *cand = reinterpret_cast<int64_t *>(take(z.refills * 64));
+  uint8_t *amask = take(z.refills);
+  uint32_t *elocal = reinterpret_cast<uint32_t *>(take(z.refills * 4));
+  uint32_t *tsum = reinterpret_cast<uint32_t *>(take((size_t)z.tiles * 4));
+  uint32_t *cstart = reinterpret_cast<uint32_t *>(take((z.calls + z.nstreams) * 4));
   const double kinv = kinv_of(sig);
-  const uint32_t total = nstreams * R;
   const uint32_t grid =
-      (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (total + kCandThreads - 1) / kCandThreads);
-  {
+      (uint32_t)std::min<uint64_t>((uint64_t)num_sms, (z.refills + kCandThreads - 1) / kCandThreads);
+  if (grid > 0) {
     ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
     if (sig == 0)
-      k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
-                                                                         d_status);
+      k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
     else if (sig == 1)
-      k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
-                                                                         d_status);
+      k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
     else
-      k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, nstreams, R, kinv, cand, amask,
-                                                                        d_status);
+      k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
   }
   CUFE_CUDA(cudaGetLastError());
-  {
+  if (z.tiles) {
     ProfScope ps("sample_scan", s);
-    k_scan_tiles<<<dim3(tiles, nstreams), 512, 0, s>>>(amask, R, tiles, elocal, tsum);
-    k_scan_sums<<<nstreams, 1024, 0, s>>>(tsum, tiles);
+    k_scan_tiles<<<z.tiles, 512, 0, s>>>(amask, sg, elocal, tsum);
+    k_scan_sums<<<z.nstreams, 1024, 0, s>>>(tsum, sg);
   }
-  const uint32_t guess = (uint32_t)((double)n / mean_accept(sig));
   {
     ProfScope ps("sample_walk", s);
-    k_walk<<<(nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, R, tiles, calls, n, guess, nstreams, cstart,
-                                              d_status);
+    k_walk<<<(z.nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), cstart, d_status);
   }
   CUFE_CUDA(cudaGetLastError());
-  out->cand = cand;
-  out->amask = amask;
-  out->call_start = cstart;
-  out->refills = R;
-  out->elocal = elocal;
-  out->tile_off = tsum;
-  out->tiles = tiles;
+  if (out) {
+    out->cand = cand;
+    out->amask = amask;
+    out->call_start = cstart;
+    out->elocal = elocal;
+    out->tile_off = tsum;
+    out->sg = sg;
+  }
+  if (d_out && z.calls) {
+    ProfScope ps_sc("sample_scatter", s);
+    k_scatter<<<(uint32_t)z.calls, 256, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
+    CUFE_CUDA(cudaGetLastError());
+  }
   return CUFE_OK;
+}
+
+// the uniform case: nstreams equal streams, tables built on the device (capturable)
+static int seg_uniform(uint32_t nstreams, uint32_t calls, uint32_t n, int sig, void *ws, cudaStream_t s, SegDev *sg,
+                       SegSizes *z, void **scratch) {
+  const SegLayout L = seg_layout(nstreams);
+  *z = seg_uniform_sizes(nstreams, calls, n, sig);
+  if (z->refills / nstreams >= (1ull << 32) / 24) return CUFE_ERR_INVALID;  // AES counter range
+  uint8_t *b = static_cast<uint8_t *>(ws);
+  *sg = seg_bind(b, nstreams);
+  const uint32_t R = (uint32_t)(z->refills / nstreams);
+  k_seg_uniform<<<(nstreams + 256) / 256, 256, 0, s>>>(
+      nstreams, calls, n, R, z->tiles / nstreams, (uint64_t)calls * 3 * n, reinterpret_cast<uint32_t *>(b + L.n),
+      reinterpret_cast<uint32_t *>(b + L.calls), reinterpret_cast<uint64_t *>(b + L.roff),
+      reinterpret_cast<uint32_t *>(b + L.toff), reinterpret_cast<uint64_t *>(b + L.coff),
+      reinterpret_cast<uint64_t *>(b + L.ooff));
+  CUFE_CUDA(cudaGetLastError());
+  *scratch = b + L.bytes;
+  return CUFE_OK;
+}
+
+int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
+                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
+  SegDev sg;
+  SegSizes z;
+  void *scratch;
+  int rc = seg_uniform(nstreams, calls, n, sig, ws, s, &sg, &z, &scratch);
+  if (rc) return rc;
+  return sample_cpu_map_seg(sig, sg, z, d_rkeys, nullptr, scratch, d_status, num_sms, s, out);
 }
 
 int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
                    uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s) {
-  CpuMapCandidates cm;
-  int rc = sample_cpu_map_candidates(sig, nstreams, d_rkeys, calls, n, ws, d_status, num_sms, s, &cm);
+  SegDev sg;
+  SegSizes z;
+  void *scratch;
+  int rc = seg_uniform(nstreams, calls, n, sig, ws, s, &sg, &z, &scratch);
   if (rc) return rc;
-  ProfScope ps_sc("sample_scatter", s);
-  k_scatter<<<dim3(calls, nstreams), 256, 0, s>>>(cm.cand, cm.amask, cm.elocal, cm.tile_off, cm.call_start,
-                                                  cm.refills, cm.tiles, calls, n, mod_args(), d_out);
-  CUFE_CUDA(cudaGetLastError());
-  return CUFE_OK;
+  return sample_cpu_map_seg(sig, sg, z, d_rkeys, d_out, scratch, d_status, num_sms, s, nullptr);
 }
 
 int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npolys, uint32_t n, uint32_t *d_out,

@@ -24,20 +24,48 @@ size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, in
 int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
                    uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s);
 
-// The candidate form of the CPU mapping, for consumers that gather the samples themselves:
-// cand[stream][refill][8] signed candidates, amask[stream][refill] accept bits and
-// call_start[stream][calls+1] (refill index where each call starts; the last entry is the
-// end of the last call).  Sample j of call c is the j-th accepted candidate of refills
-// call_start[c] .. call_start[c+1]-1, in order.
+// Segmented form: S CPU-mapping streams of different lengths.  Stream s runs calls[s]
+// sampler calls of n[s] samples; its refills occupy [roff[s], roff[s+1]) of the flattened
+// refill space, its scan tiles [toff[s], toff[s+1]), its call starts
+// call_start[coff[s] + s .. coff[s+1] + s] (calls + 1 entries), and the scatter writes its
+// residues to out[ooff[s] + c * 3 n[s] ...][3][n[s]].  Round keys rkeys[s][60].
+struct SegDev {
+  uint32_t nstreams;
+  const uint32_t *n, *calls, *toff;
+  const uint64_t *roff, *coff, *ooff;
+};
+struct SegSizes {
+  uint32_t nstreams;
+  uint64_t refills;
+  uint32_t tiles;
+  uint64_t calls;
+};
+struct SegLayout {
+  size_t n, calls, toff, roff, coff, ooff, bytes;
+};
+// the tables of S streams in one buffer (device or host, same layout)
+SegLayout seg_layout(uint32_t S);
+SegDev seg_bind(void *base, uint32_t S);
+// host: fill the tables (refills per stream from cpu_map_refills) into a host buffer of
+// seg_layout(S).bytes; ooff may be NULL (candidates only)
+SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_t *n, const uint64_t *ooff,
+                       void *host_base);
+size_t seg_scratch_bytes(const SegSizes &z);
+
+// The candidate form, for consumers that gather the samples themselves: cand[g][8] signed
+// candidates and amask[g] accept bits of flattened refill g; sample j of call c of stream s
+// is the j-th accepted candidate of refills call_start[..c] .. call_start[..c+1]-1.
 struct CpuMapCandidates {
   const int64_t *cand;
   const uint8_t *amask;
   const uint32_t *call_start;
-  uint32_t refills;  // per stream
-  // per-stream exclusive prefix of accept counts: elocal[t] + tile_off[t / 4096]
-  const uint32_t *elocal, *tile_off;
-  uint32_t tiles;
+  const uint32_t *elocal, *tile_off;  // exclusive prefix of accept counts: elocal[g] + tile_off[tile]
+  SegDev sg;
 };
+// segmented run: candidates, scan, walk, and (d_out != NULL) the scatter; out (optional)
+// receives the candidate form
+int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint32_t *d_rkeys, uint32_t *d_out,
+                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out);
 int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
                               void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out);
 

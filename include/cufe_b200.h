@@ -175,6 +175,18 @@ int cufe_ring_info(const cufe_ring *ring, uint32_t *primes, uint32_t *roots, uin
 /* in place on d_data[npoly][k][n]; forward: natural -> bit-reversed order */
 int cufe_ntt_forward(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
 int cufe_ntt_inverse(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
+/* Kernel variants and their tuner.  Variant 1: one residue polynomial per thread group,
+ * one group per residue.  Variant 2: two residues of the same modulus (rows 2t and 2t+1)
+ * per group, sharing twiddle loads and shared-memory addresses.  Variant 3: persistent
+ * groups (a grid of one wave) that load their next residue into registers while
+ * transforming the current one.  cufe_ring_tune times the three variants in both directions
+ * on a scratch buffer of npoly polynomials (capped at 1 GiB, allocated and freed inside the
+ * call, synchronous) and keeps the fastest per direction; ms (optional) receives
+ * {fwd v1, v2, v3, inv v1, v2, v3} in milliseconds per launch.  A new ring uses variant 1.
+ * No counterpart in the reference. */
+int cufe_ring_tune(cufe_ring *ring, long long npoly, float *ms, void *stream);
+int cufe_ring_set_variant(cufe_ring *ring, int fwd, int inv);
+int cufe_ring_get_variant(const cufe_ring *ring, int *fwd, int *inv);
 
 #ifdef __cplusplus
 }

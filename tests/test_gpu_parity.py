@@ -31,11 +31,14 @@ def ctx_small(oracle_built):
     c.close()
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("n", [16, 64, 256, 1024, 2048, 4096, 8192])
 @pytest.mark.parametrize("k", [3, 6])
-def test_ntt_roundtrip_and_values(n, k, rng, oracle_built):
+def test_ntt_roundtrip_and_values(n, k, variant, rng, oracle_built):
     ring = cf.Ring(n, k)
-    npoly = 5
+    ring.set_variant(variant, variant)
+    assert ring.variant == (variant, variant)
+    npoly = 5  # odd: variant 2 leaves one residue pair half empty
     q = ring.primes.astype(np.uint64)
     a = (rng.integers(0, 2**31, (npoly, k, n), dtype=np.uint64) % q[None, :, None]).astype(np.uint32)
     d = dev(a)
@@ -47,6 +50,20 @@ def test_ntt_roundtrip_and_values(n, k, rng, oracle_built):
             ref = a[p, m].copy()
             O.or_ntt_generic(ref, n, int(q[m]), np.ascontiguousarray(ring.psi[m]), 0, 0)
             assert (got[p, m] == ref).all(), (n, k, p, m)
+    ring.inverse(d)
+    assert (cf.u32(d) == a).all()
+
+
+def test_ring_tune(rng):
+    ring = cf.Ring(4096, 3)
+    t = ring.tune(64)
+    assert all(v > 0 for v in t["fwd"] + t["inv"])
+    best = (1 + int(np.argmin(t["fwd"])), 1 + int(np.argmin(t["inv"])))
+    assert ring.variant == best == t["variant"]
+    q = ring.primes.astype(np.uint64)
+    a = (rng.integers(0, 2**31, (7, 3, 4096), dtype=np.uint64) % q[None, :, None]).astype(np.uint32)
+    d = dev(a)
+    ring.forward(d)
     ring.inverse(d)
     assert (cf.u32(d) == a).all()
 
