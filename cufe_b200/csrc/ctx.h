@@ -12,7 +12,6 @@
 
 namespace cufe {
 
-typedef unsigned __int128 u128;
 
 // An RNS ring Z_q[X]/(X^n + 1) with device twiddle tables.
 struct Ring {
@@ -61,6 +60,9 @@ int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s);
 
 int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,
                       uint32_t *d_msk, cudaStream_t s);
+// setup of one instance of length l (c.l is only the context's default length)
+int ctx_setup_cpu_map_l(Ctx &c, int l, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e,
+                        uint32_t *d_mpk, uint32_t *d_msk, cudaStream_t s);
 int ctx_setup_gpu_map(Ctx &c, const uint8_t *seed2, const uint8_t *seed3, uint32_t *d_mpk, uint32_t *d_msk,
                       cudaStream_t s);
 int ctx_encrypt_cpu_map(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,

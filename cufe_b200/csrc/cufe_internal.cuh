@@ -13,6 +13,8 @@
 
 namespace cufe {
 
+typedef unsigned __int128 u128;
+
 constexpr int kMaxModuli = 6;
 constexpr int kMaxLogN = 13;
 

@@ -12,6 +12,7 @@
 
 #include "ctx.h"
 #include "ntt.cuh"
+#include "scheme.cuh"
 #include "sampler_host.h"
 #include "prof.h"
 
@@ -167,28 +168,6 @@ void Ring::release() {
 // ================================================================== NTT kernels
 
 namespace {
-
-template <int LOGN>
-constexpr int ppc() {  // residue polynomials per CTA (>= 256 threads per CTA)
-  return NttPlan<LOGN>::T >= 256 ? 1 : 256 / NttPlan<LOGN>::T;
-}
-
-__device__ __forceinline__ void load16(const uint32_t *p, uint32_t (&a)[16]) {
-  const uint4 *v = reinterpret_cast<const uint4 *>(p);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const uint4 t = v[i];
-    a[4 * i] = t.x;
-    a[4 * i + 1] = t.y;
-    a[4 * i + 2] = t.z;
-    a[4 * i + 3] = t.w;
-  }
-}
-__device__ __forceinline__ void store16(uint32_t *p, const uint32_t (&a)[16]) {
-  uint4 *v = reinterpret_cast<uint4 *>(p);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) v[i] = make_uint4(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]);
-}
 
 // MODE 0 forward, 1 forward + Shoup companions into sh, 2 inverse.  data holds `rows`
 // polynomials of k residues ([row][k][n]); a thread group transforms PP residues of one
@@ -394,20 +373,6 @@ int launch_ntt(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres,
 
 // ================================================================== scheme kernels
 
-struct SchemeArgs {
-  RingArgs ra;
-  int l;
-  uint32_t delta_mod[3], delta_sh[3];
-  uint64_t mu[3];
-};
-
-__device__ __forceinline__ uint32_t y_residue(uint32_t y, int y_signed, uint32_t q, uint64_t mu) {
-  if (!y_signed) return mod_u64(y, mu, q);
-  const int32_t ys = (int32_t)y;
-  if (ys >= 0) return mod_u64((uint64_t)ys, mu, q);
-  const uint32_t r = mod_u64((uint64_t)(-(int64_t)ys), mu, q);
-  return r ? q - r : 0u;
-}
 
 // mpk_i = a^ * NTT(s_i) + e^_i for residue polynomials r = 3i + m (src/rlwe_sife.c:69-76)
 template <int LOGN>
@@ -597,45 +562,6 @@ __global__ void __launch_bounds__(512)
   }
 }
 
-struct DecodeArgs {
-  uint32_t q0, q1, q2;
-  uint32_t c1, c1_sh, c2, c2_sh;
-  uint64_t mu2;
-  uint64_t q01;
-  unsigned long long qlo, qhi, hlo, hhi;  // q and floor(q/2) as 128-bit halves
-  uint32_t p;
-  int n;
-};
-
-// crt_reverse_gmp + round_extract_gmp (src/crt.c:46-81, src/rlwe_sife.c:288-332): Garner
-// to x in [0, q), then floor(p x / q) + (remainder > floor(q/2)).
-__device__ __forceinline__ uint32_t decode_one(uint32_t v0, uint32_t v1, uint32_t v2, const DecodeArgs &d) {
-  const uint32_t t1 = mod_red1(v1 + d.q1 - v0 % d.q1, d.q1);
-  const uint32_t u1 = shoup_mul(t1, d.c1, d.c1_sh, d.q1);
-  const uint64_t x1 = (uint64_t)v0 + (uint64_t)d.q0 * u1;
-  const uint32_t xm = mod_u64(x1, d.mu2, d.q2);
-  const uint32_t t2 = mod_red1(v2 + d.q2 - xm, d.q2);
-  const uint32_t u2 = shoup_mul(t2, d.c2, d.c2_sh, d.q2);
-  const u128 Q = ((u128)d.qhi << 64) | d.qlo, H = ((u128)d.hhi << 64) | d.hlo;
-  const u128 x = (u128)x1 + (u128)d.q01 * u2;
-  const u128 a = x * d.p;
-  // quotient < p + 1: estimate in double, correct exactly
-  long long qe = (long long)floor((double)x / (double)Q * (double)d.p);
-  if (qe < 0) qe = 0;
-  u128 prod = (u128)qe * Q;
-  while (prod > a) {
-    --qe;
-    prod -= Q;
-  }
-  u128 rem = a - prod;
-  while (rem >= Q) {
-    ++qe;
-    rem -= Q;
-  }
-  if (rem > H) ++qe;
-  return (uint32_t)qe;
-}
-
 __global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff, uint32_t *__restrict__ out,
                          DecodeArgs d) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -645,17 +571,6 @@ __global__ void k_decode(const uint32_t *__restrict__ dy, int count, int ncoeff,
   out[gid] = decode_one(v[0], v[d.n], v[2 * (size_t)d.n], d);
 }
 
-// sum over the CTA of one u64 per thread (values < 2^40); red: blockDim.x/32 words
-__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, uint64_t *red) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  uint64_t t = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-  __syncthreads();
-  return t;
-}
 
 // Constant-coefficient decryption and decode.  The reference decodes only coefficient 0 of
 // d_y (src/rlwe_sife.c:380, main.c:205 and 326), so per (ciphertext, key) and modulus
@@ -874,8 +789,9 @@ static int dispatch_logn(int logn, F &&f) {
 }
 
 // shared tail of both setups: a^ = NTT(a) in place, e^ = NTT(e), mpk_i = a^ NTT(s_i) + e^_i
-static int setup_tail(Ctx &c, uint32_t *d_mpk, const uint32_t *d_msk, uint32_t *e, uint32_t *a_sh, cudaStream_t s) {
-  const int n = c.n, l = c.l;
+static int setup_tail(Ctx &c, int l, uint32_t *d_mpk, const uint32_t *d_msk, uint32_t *e, uint32_t *a_sh,
+                      cudaStream_t s) {
+  const int n = c.n;
   uint32_t *ahat = d_mpk + (size_t)l * 3 * n;
   int rc = ntt_fwd_shoup_launch(c.ring.args, ahat, a_sh, 3, s);
   if (rc) return rc;
@@ -896,7 +812,13 @@ static int setup_tail(Ctx &c, uint32_t *d_mpk, const uint32_t *d_msk, uint32_t *
 
 int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,
                       uint32_t *d_msk, cudaStream_t s) {
-  const int n = c.n, l = c.l;
+  return ctx_setup_cpu_map_l(c, c.l, seed_a, seed_s, seed_e, d_mpk, d_msk, s);
+}
+
+int ctx_setup_cpu_map_l(Ctx &c, int l, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e,
+                        uint32_t *d_mpk, uint32_t *d_msk, cudaStream_t s) {
+  if (l < 1 || !seed_a || !seed_e) return CUFE_ERR_INVALID;
+  const int n = c.n;
   const size_t poly = (size_t)3 * n;
   const size_t samp_ws = cpu_map_workspace_bytes(2, l, n, 0);
   int rc = c.ensure_ws(samp_ws + (2 * l + 2) * poly * 4 + 4096 + 4 * 60 * 4);
@@ -916,7 +838,7 @@ int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, cons
   rc = sample_cpu_map(0, 2, rk + 60, l, n, se, sws, c.d_status, c.num_sms, s);
   if (rc) return rc;
   CUFE_CUDA(cudaMemcpyAsync(d_msk, se, (size_t)l * poly * 4, cudaMemcpyDeviceToDevice, s));
-  return setup_tail(c, d_mpk, d_msk, se + (size_t)l * poly, a_sh, s);
+  return setup_tail(c, l, d_mpk, d_msk, se + (size_t)l * poly, a_sh, s);
 }
 
 int ctx_setup_gpu_map(Ctx &c, const uint8_t *seed2, const uint8_t *seed3, uint32_t *d_mpk, uint32_t *d_msk,
@@ -937,7 +859,7 @@ int ctx_setup_gpu_map(Ctx &c, const uint8_t *seed2, const uint8_t *seed3, uint32
   if (rc) return rc;
   rc = sample_gpu_map(0, rk + 60, 0, l, n, e, c.d_status, s);
   if (rc) return rc;
-  return setup_tail(c, d_mpk, d_msk, e, a_sh, s);
+  return setup_tail(c, l, d_mpk, d_msk, e, a_sh, s);
 }
 
 static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint32_t *rhat,

@@ -15,6 +15,7 @@
 #include "aes.cuh"
 #include "sampler.cuh"
 #include "sampler_host.h"
+#include "scheme.cuh"
 #include "prof.h"
 
 #include <algorithm>
@@ -103,18 +104,6 @@ __host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : w - 12; 
 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
 constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed with p < 1e-7
-
-// stream of a flattened index: the s with off[s] <= g < off[s+1] (off non-decreasing, size S+1)
-template <typename T>
-__device__ __forceinline__ uint32_t seg_find(const T *__restrict__ off, uint32_t nseg, uint64_t g) {
-  uint32_t lo = 0, hi = nseg;  // off[lo] <= g < off[hi]
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if ((uint64_t)__ldg(off + mid) <= g) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
 
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)
