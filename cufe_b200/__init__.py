@@ -72,6 +72,15 @@ def lib():
             "cufe_ntt_forward": [vp, vp, ll, vp],
             "cufe_ntt_inverse": [vp, vp, ll, vp],
             "cufe_ring_tune": [vp, ll, vp, vp],
+            "cufe_batch_create": [C.POINTER(vp), i, vp, vp, C.c_size_t, i],
+            "cufe_batch_destroy": [vp],
+            "cufe_batch_setup": [vp, vp, vp, vp, vp],
+            "cufe_batch_bind": [vp, vp, vp, vp, vp, vp, vp],
+            "cufe_batch_run": [vp, vp],
+            "cufe_batch_replay": [vp, vp],
+            "cufe_batch_status": [vp],
+            "cufe_batch_info": [vp, vp, vp, vp, vp],
+            "cufe_batch_instance": [vp, i, vp, vp, vp, vp],
             "cufe_ring_set_variant": [vp, i, i],
             "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
@@ -136,9 +145,17 @@ def _dev(shape, device):
 
 
 def to_dev(a, device="cuda"):
+    """uint32 words on the device (int32 tensor of the same bits)"""
     import torch
     a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
     return torch.from_numpy(a.view(np.int32)).to(device)
+
+
+def bytes_to_dev(a, device="cuda"):
+    """bytes (seeds) on the device, unchanged: a uint8 tensor"""
+    import torch
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint8))
+    return torch.from_numpy(a).to(device)
 
 
 class Context:
@@ -352,3 +369,85 @@ class Ring:
 
     def set_variant(self, fwd, inv):
         _check(lib().cufe_ring_set_variant(self.h, fwd, inv), "cufe_ring_set_variant")
+
+
+class Batch:
+    """Many independent IPFE instances of different (n_i, l_i), each with its own master key
+    pair, stepped together: encrypt x_i, keygen y_i (signed), decrypt and decode the
+    inner product (coefficient 0 of d_y, in [0, p_i], p_i = 64 l_i + 1)."""
+
+    def __init__(self, n, l, max_chunk_bytes=0, device=0):
+        import torch
+        self.n = np.ascontiguousarray(n, np.int32)
+        self.l = np.ascontiguousarray(l, np.int32)
+        assert self.n.shape == self.l.shape and self.n.ndim == 1
+        self.count, self.device = len(self.n), device
+        self.dev = torch.device("cuda", device)
+        h = C.c_void_p()
+        _check(lib().cufe_batch_create(C.byref(h), self.count, self.n.ctypes.data, self.l.ctypes.data,
+                                       max_chunk_bytes, device), "cufe_batch_create")
+        self.h = h
+        self.x_off = np.zeros(self.count + 1, np.uint64)
+        ch, kb, sb = C.c_int(0), C.c_size_t(0), C.c_size_t(0)
+        _check(lib().cufe_batch_info(h, self.x_off.ctypes.data, C.byref(ch), C.byref(kb), C.byref(sb)),
+               "cufe_batch_info")
+        self.chunks, self.key_bytes, self.scratch_bytes = ch.value, kb.value, sb.value
+        self._bound = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cufe_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self, seeds_a, seeds_s, seeds_e, stream=None):
+        a, s_, e = _seeds(seeds_a), _seeds(seeds_s), _seeds(seeds_e)
+        _check(lib().cufe_batch_setup(self.h, _ptr(a), _ptr(s_), _ptr(e), _stream(stream, self.device)),
+               "cufe_batch_setup")
+
+    def pack(self, rows):
+        """concatenate per-instance vectors (instance i of length l_i) in the batch's layout"""
+        return np.concatenate([np.asarray(r).reshape(-1) for r in rows])
+
+    def bind(self, x, y, seeds2, seeds3, out=None, d0=None):
+        """device tensors: x uint32/int32 [sum l], y int32 [sum l], seeds [count][32] uint8"""
+        import torch
+        for t in (seeds2, seeds3):
+            if t.dtype != torch.uint8 or t.numel() != 32 * self.count:
+                raise ValueError("seeds must be uint8 device tensors of [count][32] bytes")
+        out = torch.empty(self.count, dtype=torch.int32, device=self.dev) if out is None else out
+        _check(lib().cufe_batch_bind(self.h, _ptr(x), _ptr(y), _ptr(seeds2), _ptr(seeds3), _ptr(out), _ptr(d0)),
+               "cufe_batch_bind")
+        self._bound = (x, y, seeds2, seeds3, out, d0)  # keep the buffers alive
+        return out
+
+    def run(self, stream=None):
+        _check(lib().cufe_batch_run(self.h, _stream(stream, self.device)), "cufe_batch_run")
+
+    def replay(self, stream=None):
+        _check(lib().cufe_batch_replay(self.h, _stream(stream, self.device)), "cufe_batch_replay")
+
+    def status(self):
+        _check(lib().cufe_batch_status(self.h), "cufe_batch_status")
+
+    def instance(self, i):
+        """(mpk, msk, sky, ct) device addresses of instance i (ct None unless available)"""
+        ptrs = [C.c_void_p() for _ in range(4)]
+        _check(lib().cufe_batch_instance(self.h, i, *[C.byref(p) for p in ptrs]), "cufe_batch_instance")
+        return tuple(p.value for p in ptrs)
+
+    def fetch(self, addr, words):
+        """copy `words` uint32 from a device address of this batch into a numpy array"""
+        import torch
+
+        class _View:  # a device range exposed through __cuda_array_interface__ (no copy)
+            __cuda_array_interface__ = {"shape": (words,), "typestr": "<i4", "data": (addr, False), "version": 2}
+
+        t = torch.as_tensor(_View(), device=self.dev)
+        torch.cuda.synchronize(self.dev)
+        return t.cpu().numpy().view(np.uint32)

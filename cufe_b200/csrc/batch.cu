@@ -1,0 +1,687 @@
+// batch.cu -- heterogeneous batches of IPFE instances.
+//
+// A batch holds `count` independent instances of the scheme (src/rlwe_sife.c:32-286), each
+// with its own ring degree n_i, vector length l_i (so its own p_i = 64 l_i + 1 and
+// Delta_i = floor(q / p_i), src/params.h:26-27) and its own master key pair, resident on the
+// device.  One step runs, for every instance, encrypt(x_i) with the CPU stream mapping
+// (per-instance seeds), keygen(y_i), decryption and decode of coefficient 0 -- the
+// inner product -- as a fixed sequence of launches over all instances at once:
+//
+//   keys:     device AES-256 key expansion of every instance's two seeds
+//   keygen:   one launch over (instance, modulus, 256 coefficients) units
+//   per chunk of instances (scratch bounded by max_chunk_bytes):
+//     sigma_2 sampler over all chunk streams (segmented CPU mapping: 2 calls of n_i each)
+//     r^ = NTT(r) per ring degree
+//     sigma_3 sampler over all chunk streams (l_i calls of n_i each)
+//     encryption: one launch per ring degree over every (instance, slot, modulus) residue
+//     constant-coefficient decryption + decode, one CTA per instance
+//
+// Instances are kept in ring-degree order internally (stable); inputs and outputs use the
+// caller's order.  Every table the launches read is built once at creation, so a step is
+// free of host work and can be captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+#include "ntt.cuh"
+#include "prof.h"
+#include "sampler_host.h"
+#include "scheme.cuh"
+
+namespace cufe {
+
+struct InstDev {
+  uint64_t mpk, msk, sky;    // word offsets: key arena, function-key arena
+  uint64_t ct, f3, s2o, rh;  // word offsets in the chunk arenas
+  uint64_t x;                // word offset of x_i and y_i in the packed inputs
+  uint32_t l, n, user, p;
+  uint32_t delta_mod[3], delta_sh[3];
+};
+
+struct ModQ {
+  uint32_t q[3];
+  uint64_t mu[3];
+};
+
+namespace {
+
+// sk_i[m][c] = sum_{j < l_i} (y_ij mod q_m) msk_i[j][m][c] (src/rlwe_sife.c:215-245); one CTA
+// per (instance, modulus, 256 coefficients)
+__global__ void __launch_bounds__(256)
+    k_keygen_het(const InstDev *__restrict__ inst, const uint64_t *__restrict__ unit_off, uint32_t count,
+                 const uint32_t *__restrict__ keys, const int32_t *__restrict__ y, uint32_t *__restrict__ sky,
+                 ModQ mq) {
+  extern __shared__ uint32_t smem_u32[];
+  const uint32_t i = seg_find(unit_off, count, blockIdx.x);
+  const InstDev I = inst[i];
+  const uint32_t local = blockIdx.x - (uint32_t)unit_off[i], chunks = I.n / 256;
+  const int m = (int)(local / chunks);
+  const uint32_t col = (local - m * chunks) * 256 + threadIdx.x;
+  const uint32_t q = mq.q[m];
+  uint32_t *yq = smem_u32, *ys = smem_u32 + I.l;
+  for (uint32_t j = threadIdx.x; j < I.l; j += blockDim.x) {
+    const uint32_t v = y_residue((uint32_t)y[I.x + j], 1, q, mq.mu[m]);
+    yq[j] = v;
+    ys[j] = (uint32_t)(((uint64_t)v << 32) / q);
+  }
+  __syncthreads();
+  const uint32_t *mk = keys + I.msk + (size_t)m * I.n + col;
+  uint64_t acc = 0;
+  for (uint32_t j = 0; j < I.l; ++j) acc += shoup_lazy(__ldg(mk + (size_t)j * 3 * I.n), yq[j], ys[j], q);
+  sky[I.sky + (size_t)m * I.n + col] = mod_u64(acc, mq.mu[m], q);
+}
+
+// encryption of every residue (instance, slot j <= l_i, modulus m) of one ring degree
+// (src/rlwe_sife.c:157-176): c = INTT(pk_j r^) + f + Delta_i x_ij, with f = f_j (sigma_3) for
+// j < l_i and f_0 (the second sigma_2 call) for the last slot
+template <int LOGN>
+__global__ void __launch_bounds__(512)
+    k_encrypt_het(const InstDev *__restrict__ inst, const uint64_t *__restrict__ res_off, uint32_t cnt,
+                  long long nres, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ rh,
+                  const uint32_t *__restrict__ rh_sh, const uint32_t *__restrict__ f3,
+                  const uint32_t *__restrict__ s2o, const uint32_t *__restrict__ x, uint32_t *__restrict__ ct,
+                  RingArgs ra, ModQ mq) {
+  using P = NttPlan<LOGN>;
+  extern __shared__ uint32_t smem_u32[];
+  const int th = threadIdx.x;
+  const long long wi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool act = wi < nres;
+  const long long ww = act ? wi : nres - 1;
+  const uint32_t i = seg_find(res_off, cnt, (uint64_t)ww);
+  const InstDev &I = inst[i];
+  const uint32_t local = (uint32_t)(ww - (long long)res_off[i]);
+  const uint32_t j = local / 3, l = I.l;
+  const int m = (int)(local - j * 3);
+  const uint32_t q = ra.q[m];
+  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t a[16], w[16], wsh[16];
+  load16(keys + I.mpk + (size_t)local * P::N + th * 16, a);
+  load16(rh + I.rh + (size_t)m * P::N + th * 16, w);
+  load16(rh_sh + I.rh + (size_t)m * P::N + th * 16, wsh);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
+  ntt_inv_core<LOGN>(a, sm, th, q, ra.ipsi2 + (size_t)m * P::N, ra.ninv[m], ra.ninv_sh[m], ra.w1n[m],
+                     ra.w1n_sh[m]);
+  const uint32_t *f;
+  uint32_t msg = 0;
+  if (j < l) {
+    f = f3 + I.f3 + (size_t)local * P::N;
+    const uint32_t xr = mod_u64(x[I.x + j], mq.mu[m], q);
+    msg = shoup_mul(xr, I.delta_mod[m], I.delta_sh[m], q);
+  } else {
+    f = s2o + I.s2o + (size_t)(3 + m) * P::N;
+  }
+  uint32_t *c = ct + I.ct + (size_t)local * P::N;
+  if (act) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const int jj = P::template idx<0>(th, e);
+      c[jj] = mod_add(mod_add(a[e], f[jj], q), msg, q);
+    }
+  }
+}
+
+// d_y[0] = sum_j y_j c_j[0] - (c_l[0] sk[0] - sum_{t>=1} c_l[t] sk[n-t]) per modulus, then the
+// reference's decode with this instance's p (src/rlwe_sife.c:248-332): one CTA per instance
+__global__ void __launch_bounds__(256)
+    k_dec_coef0_het(const InstDev *__restrict__ inst, const uint32_t *__restrict__ ct,
+                    const uint32_t *__restrict__ sky, const int32_t *__restrict__ y, uint32_t *__restrict__ out,
+                    uint32_t *__restrict__ d0, ModQ mq, DecodeArgs dd) {
+  __shared__ uint64_t red[8];
+  const InstDev I = inst[blockIdx.x];
+  const uint32_t n = I.n, l = I.l;
+  const uint32_t *cb = ct + I.ct;
+  uint32_t r[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const uint32_t q = mq.q[m];
+    const uint64_t mu = mq.mu[m];
+    uint64_t mac = 0, neg = 0;
+    for (uint32_t j = threadIdx.x; j < l; j += blockDim.x) {
+      const uint32_t yv = y_residue((uint32_t)y[I.x + j], 1, q, mu);
+      mac += mod_u64((uint64_t)cb[((size_t)j * 3 + m) * n] * yv, mu, q);
+    }
+    const uint32_t *cl = cb + ((size_t)l * 3 + m) * n;
+    const uint32_t *sk = sky + I.sky + (size_t)m * n;
+    for (uint32_t t = threadIdx.x + 1; t < n; t += blockDim.x) neg += mod_u64((uint64_t)cl[t] * sk[n - t], mu, q);
+    const uint64_t macs = block_sum_u64(mac, red), negs = block_sum_u64(neg, red);
+    const uint32_t c0s0 = mod_u64((uint64_t)cl[0] * sk[0], mu, q);
+    r[m] = mod_add(mod_sub(mod_u64(macs, mu, q), c0s0, q), mod_u64(negs, mu, q), q);
+  }
+  if (threadIdx.x == 0) {
+    if (d0)
+      for (int m = 0; m < 3; ++m) d0[(size_t)I.user * 3 + m] = r[m];
+    DecodeArgs d = dd;
+    d.p = I.p;
+    d.n = (int)n;
+    out[I.user] = decode_one(r[0], r[1], r[2], d);
+  }
+}
+
+template <class F>
+int dispatch_logn_b(int logn, F &&f) {
+  switch (logn) {
+    case 8: return f(std::integral_constant<int, 8>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 10: return f(std::integral_constant<int, 10>());
+    case 11: return f(std::integral_constant<int, 11>());
+    case 12: return f(std::integral_constant<int, 12>());
+    case 13: return f(std::integral_constant<int, 13>());
+  }
+  return CUFE_ERR_INVALID;
+}
+
+size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------- host side
+
+struct BatchGroup {  // instances of one ring degree inside a chunk
+  int logn = 0;
+  uint32_t first = 0, count = 0;  // chunk-local instance range
+  uint64_t rh = 0, s2o = 0;       // word offsets of the group in the chunk arenas
+  long long nres = 0;             // residues to encrypt: sum (l_i + 1) * 3
+  size_t inst_off = 0, res_off = 0;  // byte offsets of its tables in the table blob
+};
+
+struct BatchChunk {
+  uint32_t first = 0, count = 0;  // internal-order instance range
+  std::vector<BatchGroup> groups;
+  size_t inst_off = 0;            // byte offset of the chunk's InstDev[count]
+  size_t seg2_off = 0, seg3_off = 0;
+  SegSizes z2{}, z3{};
+};
+
+struct Batch {
+  int device = 0, count = 0, num_sms = 148;
+  std::vector<int> n, l;         // caller order
+  std::vector<uint32_t> order;   // internal position -> caller index
+  std::vector<uint64_t> x_off;   // caller order, count + 1
+  std::map<int, std::unique_ptr<Ctx>> ctx;  // one context (ring, setup workspace) per n
+  std::vector<BatchChunk> chunks;
+  std::vector<InstDev> inst;     // internal order, arena offsets of the first chunk layout
+  size_t scratch_bytes = 0, key_bytes = 0;
+  // device memory
+  uint32_t *keys = nullptr, *sky = nullptr;
+  uint8_t *tables = nullptr;     // InstDev arrays, offsets, segment tables
+  uint8_t *scratch = nullptr;    // chunk arenas + sampler scratch
+  uint32_t *rk = nullptr;        // [2][count][60] round keys (internal order)
+  uint32_t *perm = nullptr;      // internal position -> caller index
+  uint32_t *status = nullptr;
+  size_t keygen_inst_off = 0, keygen_unit_off = 0;
+  uint32_t keygen_units = 0, max_l = 0;
+  // chunk arena layout (bytes)
+  size_t a_s2o = 0, a_rh = 0, a_rhsh = 0, a_f3 = 0, a_ct = 0, a_samp = 0;
+  // bound inputs / outputs
+  const uint32_t *x = nullptr;
+  const int32_t *y = nullptr;
+  const uint8_t *seeds2 = nullptr, *seeds3 = nullptr;
+  uint32_t *out = nullptr, *d0 = nullptr;
+  bool ran = false;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int last_chunk = -1;
+  ModQ mq{};
+  DecodeArgs dd{};
+
+  int create(int count_, const int *n_, const int *l_, size_t max_chunk_bytes, int dev);
+  void release();
+  int setup(const uint8_t *sa, const uint8_t *ss, const uint8_t *se, cudaStream_t s);
+  int run(cudaStream_t s);
+  int replay(cudaStream_t s);
+  void drop_graph();
+};
+
+static uint32_t delta_of(uint32_t p, int j) {
+  const u128 q = (u128)kRefPrimes[0] * kRefPrimes[1] * kRefPrimes[2];
+  return (uint32_t)((q / p) % kRefPrimes[j]);
+}
+
+int Batch::create(int count_, const int *n_, const int *l_, size_t max_chunk_bytes, int dev) {
+  if (count_ < 1 || !n_ || !l_) return CUFE_ERR_INVALID;
+  count = count_;
+  device = dev;
+  n.assign(n_, n_ + count);
+  l.assign(l_, l_ + count);
+  for (int i = 0; i < count; ++i) {
+    if (n[i] < 256 || n[i] > 8192 || (n[i] & (n[i] - 1)) || l[i] < 1 || l[i] > 4096) {
+      set_last_error("batch: n must be a power of two in [256, 8192] and l in [1, 4096]");
+      return CUFE_ERR_INVALID;
+    }
+  }
+  CUFE_CUDA(cudaSetDevice(device));
+  CUFE_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  if (!max_chunk_bytes) max_chunk_bytes = (size_t)24 << 30;
+  // contexts per ring degree
+  for (int i = 0; i < count; ++i)
+    if (!ctx.count(n[i])) {
+      std::unique_ptr<Ctx> c(new Ctx);
+      int rc = c->init(n[i], l[i], device);
+      if (rc) return rc;
+      ctx[n[i]] = std::move(c);
+    }
+  const Ctx &c0 = *ctx.begin()->second;
+  for (int j = 0; j < 3; ++j) {
+    mq.q[j] = kRefPrimes[j];
+    mq.mu[j] = (uint64_t)(((u128)1 << 64) / kRefPrimes[j]);
+  }
+  dd.q0 = kRefPrimes[0];
+  dd.q1 = kRefPrimes[1];
+  dd.q2 = kRefPrimes[2];
+  dd.c1 = c0.crt_c1;
+  dd.c1_sh = c0.crt_c1_sh;
+  dd.c2 = c0.crt_c2;
+  dd.c2_sh = c0.crt_c2_sh;
+  dd.mu2 = mq.mu[2];
+  dd.q01 = (uint64_t)kRefPrimes[0] * kRefPrimes[1];
+  dd.qlo = (unsigned long long)(uint64_t)c0.q;
+  dd.qhi = (unsigned long long)(uint64_t)(c0.q >> 64);
+  dd.hlo = (unsigned long long)(uint64_t)c0.qhalf;
+  dd.hhi = (unsigned long long)(uint64_t)(c0.qhalf >> 64);
+  // caller-order packing of x / y
+  x_off.assign(count + 1, 0);
+  for (int i = 0; i < count; ++i) x_off[i + 1] = x_off[i] + l[i];
+  // internal order: by ring degree, stable
+  order.resize(count);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return n[a] < n[b]; });
+  // key arena: mpk_i [(l+1)][3][n], msk_i [l][3][n]; function keys [3][n]
+  inst.assign(count, InstDev{});
+  uint64_t kw = 0, skw = 0;
+  for (int pos = 0; pos < count; ++pos) {
+    const uint32_t u = order[pos];
+    InstDev &I = inst[pos];
+    I.l = (uint32_t)l[u];
+    I.n = (uint32_t)n[u];
+    I.user = u;
+    I.p = 64u * I.l + 1u;  // B_x * B_y * l + 1 with B_x = 4, B_y = 16 (src/params.h:26)
+    for (int j = 0; j < 3; ++j) {
+      I.delta_mod[j] = delta_of(I.p, j);
+      I.delta_sh[j] = shoup_of(I.delta_mod[j], kRefPrimes[j]);
+    }
+    I.mpk = kw;
+    kw += (uint64_t)(I.l + 1) * 3 * I.n;
+    I.msk = kw;
+    kw += (uint64_t)I.l * 3 * I.n;
+    I.sky = skw;
+    skw += (uint64_t)3 * I.n;
+    I.x = x_off[u];
+    max_l = std::max(max_l, I.l);
+  }
+  key_bytes = kw * 4;
+  // chunks: greedy in internal order under the scratch budget
+  auto inst_bytes = [&](const InstDev &I) {
+    const uint64_t poly = (uint64_t)3 * I.n * 4;
+    const uint64_t R3 = cpu_map_refills(I.l, I.n, 2), R2 = cpu_map_refills(2, I.n, 1);
+    return poly * (2 + 2 + I.l + (I.l + 1)) + R3 * 70 + R2 * 70 + 4096;
+  };
+  for (int pos = 0; pos < count;) {
+    BatchChunk ch;
+    ch.first = pos;
+    uint64_t b = 0;
+    while (pos < count && (ch.count == 0 || b + inst_bytes(inst[pos]) <= max_chunk_bytes)) {
+      b += inst_bytes(inst[pos]);
+      ++pos;
+      ++ch.count;
+    }
+    chunks.push_back(ch);
+  }
+  // per chunk: arena offsets, groups, segment tables; sizes of the largest chunk
+  std::vector<uint8_t> blob;
+  auto put = [&](const void *src, size_t bytes) {
+    const size_t off = a256(blob.size());
+    blob.resize(off + a256(bytes));
+    if (src) std::memcpy(blob.data() + off, src, bytes);
+    return off;
+  };
+  size_t m_s2o = 0, m_rh = 0, m_f3 = 0, m_ct = 0, m_samp = 0;
+  std::vector<InstDev> chunk_inst;
+  for (BatchChunk &ch : chunks) {
+    uint64_t w_s2o = 0, w_rh = 0, w_f3 = 0, w_ct = 0;
+    std::vector<uint32_t> calls2, n2, calls3, n3;
+    std::vector<uint64_t> o2, o3;
+    chunk_inst.assign(inst.begin() + ch.first, inst.begin() + ch.first + ch.count);
+    for (uint32_t k = 0; k < ch.count; ++k) {
+      InstDev &I = chunk_inst[k];
+      const int logn = __builtin_ctz(I.n);
+      if (ch.groups.empty() || ch.groups.back().logn != logn) {
+        BatchGroup g;
+        g.logn = logn;
+        g.first = k;
+        g.rh = w_rh;
+        g.s2o = w_s2o;
+        ch.groups.push_back(g);
+      }
+      BatchGroup &g = ch.groups.back();
+      ++g.count;
+      g.nres += (long long)(I.l + 1) * 3;
+      I.s2o = w_s2o;
+      I.rh = w_rh;
+      I.f3 = w_f3;
+      I.ct = w_ct;
+      calls2.push_back(2);
+      n2.push_back(I.n);
+      o2.push_back(w_s2o);
+      calls3.push_back(I.l);
+      n3.push_back(I.n);
+      o3.push_back(w_f3);
+      w_s2o += (uint64_t)6 * I.n;
+      w_rh += (uint64_t)3 * I.n;
+      w_f3 += (uint64_t)I.l * 3 * I.n;
+      w_ct += (uint64_t)(I.l + 1) * 3 * I.n;
+    }
+    // the host copy keeps the first chunk's arena offsets (ciphertext lookup of a one-chunk batch)
+    if (&ch == &chunks.front())
+      for (uint32_t k = 0; k < ch.count; ++k) inst[ch.first + k] = chunk_inst[k];
+    ch.inst_off = put(chunk_inst.data(), chunk_inst.size() * sizeof(InstDev));
+    for (BatchGroup &g : ch.groups) {
+      g.inst_off = put(chunk_inst.data() + g.first, (size_t)g.count * sizeof(InstDev));
+      std::vector<uint64_t> ro(g.count + 1, 0);
+      for (uint32_t k = 0; k < g.count; ++k) ro[k + 1] = ro[k] + (uint64_t)(chunk_inst[g.first + k].l + 1) * 3;
+      g.res_off = put(ro.data(), ro.size() * 8);
+    }
+    const SegLayout L2 = seg_layout(ch.count), L3 = seg_layout(ch.count);
+    std::vector<uint8_t> t2(L2.bytes), t3(L3.bytes);
+    ch.z2 = seg_fill_host(1, ch.count, calls2.data(), n2.data(), o2.data(), t2.data());
+    ch.z3 = seg_fill_host(2, ch.count, calls3.data(), n3.data(), o3.data(), t3.data());
+    ch.seg2_off = put(t2.data(), t2.size());
+    ch.seg3_off = put(t3.data(), t3.size());
+    m_s2o = std::max(m_s2o, (size_t)w_s2o * 4);
+    m_rh = std::max(m_rh, (size_t)w_rh * 4);
+    m_f3 = std::max(m_f3, (size_t)w_f3 * 4);
+    m_ct = std::max(m_ct, (size_t)w_ct * 4);
+    m_samp = std::max({m_samp, seg_scratch_bytes(ch.z2), seg_scratch_bytes(ch.z3)});
+  }
+  // keygen over all instances: units (instance, modulus, 256 coefficients)
+  {
+    std::vector<uint64_t> uo(count + 1, 0);
+    for (int pos = 0; pos < count; ++pos) uo[pos + 1] = uo[pos] + (uint64_t)3 * inst[pos].n / 256;
+    keygen_units = (uint32_t)uo[count];
+    // the keygen reads only key offsets, l, n and x: the first-chunk arena offsets are unused
+    keygen_inst_off = put(inst.data(), inst.size() * sizeof(InstDev));
+    keygen_unit_off = put(uo.data(), uo.size() * 8);
+  }
+  a_s2o = 0;
+  a_rh = a_s2o + a256(m_s2o);
+  a_rhsh = a_rh + a256(m_rh);
+  a_f3 = a_rhsh + a256(m_rh);
+  a_ct = a_f3 + a256(m_f3);
+  a_samp = a_ct + a256(m_ct);
+  scratch_bytes = a_samp + a256(m_samp);
+  CUFE_CUDA(cudaMalloc(&keys, std::max<size_t>(key_bytes, 256)));
+  CUFE_CUDA(cudaMalloc(&sky, std::max<size_t>(skw * 4, 256)));
+  CUFE_CUDA(cudaMalloc(&tables, std::max<size_t>(blob.size(), 256)));
+  CUFE_CUDA(cudaMemcpy(tables, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  CUFE_CUDA(cudaMalloc(&scratch, scratch_bytes));
+  CUFE_CUDA(cudaMalloc(&rk, (size_t)2 * count * 60 * 4));
+  CUFE_CUDA(cudaMalloc(&perm, (size_t)count * 4));
+  CUFE_CUDA(cudaMemcpy(perm, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice));
+  CUFE_CUDA(cudaMalloc(&status, 256));
+  CUFE_CUDA(cudaMemset(status, 0, 256));
+  return CUFE_OK;
+}
+
+void Batch::drop_graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+}
+
+void Batch::release() {
+  drop_graph();
+  if (cap) cudaStreamDestroy(cap);
+  for (void *p : {(void *)keys, (void *)sky, (void *)tables, (void *)scratch, (void *)rk, (void *)perm,
+                  (void *)status})
+    if (p) cudaFree(p);
+  keys = sky = rk = perm = status = nullptr;
+  tables = scratch = nullptr;
+  cap = nullptr;
+  for (auto &kv : ctx) kv.second->release();
+  ctx.clear();
+}
+
+int Batch::setup(const uint8_t *sa, const uint8_t *ss, const uint8_t *se, cudaStream_t s) {
+  if (!sa || !se) return CUFE_ERR_INVALID;
+  for (int pos = 0; pos < count; ++pos) {
+    const InstDev &I = inst[pos];
+    const uint32_t u = I.user;
+    int rc = ctx_setup_cpu_map_l(*ctx[(int)I.n], (int)I.l, sa + 32 * (size_t)u, ss ? ss + 32 * (size_t)u : nullptr,
+                                 se + 32 * (size_t)u, keys + I.mpk, keys + I.msk, s);
+    if (rc) return rc;
+  }
+  return CUFE_OK;
+}
+
+int Batch::run(cudaStream_t s) {
+  if (!x || !y || !seeds2 || !seeds3 || !out) {
+    set_last_error("batch: bind the inputs and outputs first");
+    return CUFE_ERR_INVALID;
+  }
+  uint32_t *rk2 = rk, *rk3 = rk + (size_t)count * 60;
+  int rc = expand_keys_device(seeds2, perm, count, rk2, s);
+  if (rc) return rc;
+  rc = expand_keys_device(seeds3, perm, count, rk3, s);
+  if (rc) return rc;
+  {
+    const size_t smem = (size_t)2 * max_l * 4;
+    static bool attr = false;
+    if (!attr) {
+      CUFE_CUDA(cudaFuncSetAttribute(k_keygen_het, cudaFuncAttributeMaxDynamicSharedMemorySize, 32 * 1024));
+      attr = true;
+    }
+    ProfScope ps("batch_keygen", s);
+    k_keygen_het<<<keygen_units, 256, smem, s>>>(reinterpret_cast<const InstDev *>(tables + keygen_inst_off),
+                                                 reinterpret_cast<const uint64_t *>(tables + keygen_unit_off),
+                                                 (uint32_t)count, keys, y, sky, mq);
+    CUFE_CUDA(cudaGetLastError());
+  }
+  uint32_t *s2o = reinterpret_cast<uint32_t *>(scratch + a_s2o);
+  uint32_t *rh = reinterpret_cast<uint32_t *>(scratch + a_rh);
+  uint32_t *rhsh = reinterpret_cast<uint32_t *>(scratch + a_rhsh);
+  uint32_t *f3 = reinterpret_cast<uint32_t *>(scratch + a_f3);
+  uint32_t *ct = reinterpret_cast<uint32_t *>(scratch + a_ct);
+  void *samp = scratch + a_samp;
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    const BatchChunk &ch = chunks[ci];
+    const SegDev sg2 = seg_bind(tables + ch.seg2_off, ch.count), sg3 = seg_bind(tables + ch.seg3_off, ch.count);
+    rc = sample_cpu_map_seg(1, sg2, ch.z2, rk2 + (size_t)ch.first * 60, s2o, samp, status, num_sms, s, nullptr);
+    if (rc) return rc;
+    for (const BatchGroup &g : ch.groups) {
+      const size_t nn = (size_t)1 << g.logn;
+      CUFE_CUDA(cudaMemcpy2DAsync(rh + g.rh, 3 * nn * 4, s2o + g.s2o, 6 * nn * 4, 3 * nn * 4, g.count,
+                                  cudaMemcpyDeviceToDevice, s));
+      rc = ntt_fwd_shoup_launch(ctx[(int)nn]->ring.args, rh + g.rh, rhsh + g.rh, (long long)g.count * 3, s);
+      if (rc) return rc;
+    }
+    rc = sample_cpu_map_seg(2, sg3, ch.z3, rk3 + (size_t)ch.first * 60, f3, samp, status, num_sms, s, nullptr);
+    if (rc) return rc;
+    for (const BatchGroup &g : ch.groups) {
+      const RingArgs &ra = ctx[1 << g.logn]->ring.args;
+      rc = dispatch_logn_b(g.logn, [&](auto LL) {
+        constexpr int LOGN = decltype(LL)::value;
+        using P = NttPlan<LOGN>;
+        constexpr int G = ppc<LOGN>();
+        static bool attr = false;
+        if (!attr) {
+          CUFE_CUDA(cudaFuncSetAttribute(k_encrypt_het<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+          attr = true;
+        }
+        ProfScope ps("batch_encrypt", s);
+        k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, s>>>(
+            reinterpret_cast<const InstDev *>(tables + g.inst_off), reinterpret_cast<const uint64_t *>(tables + g.res_off),
+            g.count, g.nres, keys, rh, rhsh, f3, s2o, x, ct, ra, mq);
+        CUFE_CUDA(cudaGetLastError());
+        return (int)CUFE_OK;
+      });
+      if (rc) return rc;
+    }
+    {
+      ProfScope ps("batch_decrypt", s);
+      k_dec_coef0_het<<<ch.count, 256, 0, s>>>(reinterpret_cast<const InstDev *>(tables + ch.inst_off), ct, sky, y,
+                                              out, d0, mq, dd);
+      CUFE_CUDA(cudaGetLastError());
+    }
+  }
+  last_chunk = (int)chunks.size() - 1;
+  ran = true;
+  return CUFE_OK;
+}
+
+int Batch::replay(cudaStream_t s) {
+  if (!exec) {
+    if (!ran) {  // first-use attribute settings and workspace happen outside the capture
+      int rc = run(s);
+      if (rc) return rc;
+      CUFE_CUDA(cudaStreamSynchronize(s));
+    }
+    if (!cap) CUFE_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    Prof *saved = t_prof;
+    t_prof = nullptr;  // no profiling events inside the graph
+    CUFE_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = run(cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cap, &g);
+    t_prof = saved;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      set_last_error(std::string("batch capture: ") + cudaGetErrorString(e));
+      return CUFE_ERR_CUDA;
+    }
+    graph = g;
+    CUFE_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  }
+  CUFE_CUDA(cudaGraphLaunch(exec, s));
+  return CUFE_OK;
+}
+
+}  // namespace cufe
+
+// ---------------------------------------------------------------------------- C ABI
+
+struct cufe_batch {
+  cufe::Batch b;
+  std::mutex mu;
+};
+
+extern "C" {
+
+int cufe_batch_create(cufe_batch **out, int count, const int *n, const int *l, size_t max_chunk_bytes, int device) {
+  if (!out) return CUFE_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cufe::set_last_error("no CUDA device");
+    return CUFE_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return CUFE_ERR_INVALID;
+  cufe_batch *h = new cufe_batch;
+  const int rc = h->b.create(count, n, l, max_chunk_bytes, device);
+  if (rc) {
+    h->b.release();
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return CUFE_OK;
+}
+
+int cufe_batch_destroy(cufe_batch *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  cudaSetDevice(h->b.device);
+  h->b.release();
+  delete h;
+  return CUFE_OK;
+}
+
+int cufe_batch_setup(cufe_batch *h, const uint8_t *seeds_a, const uint8_t *seeds_s, const uint8_t *seeds_e,
+                     void *stream) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->b.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return h->b.setup(seeds_a, seeds_s, seeds_e, static_cast<cudaStream_t>(stream));
+}
+
+int cufe_batch_bind(cufe_batch *h, const uint32_t *d_x, const int32_t *d_y, const uint8_t *d_seeds2,
+                    const uint8_t *d_seeds3, uint32_t *d_out, uint32_t *d_d0) {
+  if (!h || !d_x || !d_y || !d_seeds2 || !d_seeds3 || !d_out) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  cufe::Batch &b = h->b;
+  if (b.x != d_x || b.y != d_y || b.seeds2 != d_seeds2 || b.seeds3 != d_seeds3 || b.out != d_out || b.d0 != d_d0)
+    b.drop_graph();
+  b.x = d_x;
+  b.y = d_y;
+  b.seeds2 = d_seeds2;
+  b.seeds3 = d_seeds3;
+  b.out = d_out;
+  b.d0 = d_d0;
+  return CUFE_OK;
+}
+
+int cufe_batch_run(cufe_batch *h, void *stream) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->b.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return h->b.run(static_cast<cudaStream_t>(stream));
+}
+
+int cufe_batch_replay(cufe_batch *h, void *stream) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->b.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return h->b.replay(static_cast<cudaStream_t>(stream));
+}
+
+int cufe_batch_status(cufe_batch *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  uint32_t st = 0;
+  if (cudaSetDevice(h->b.device) != cudaSuccess || cudaMemcpy(&st, h->b.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CUFE_ERR_CUDA;
+  if (st) {
+    cufe::set_last_error("batch: sampler status " + std::to_string(st));
+    return CUFE_ERR_SAMPLER;
+  }
+  return CUFE_OK;
+}
+
+int cufe_batch_info(const cufe_batch *h, uint64_t *x_off, int *chunks, size_t *key_bytes, size_t *scratch_bytes) {
+  if (!h) return CUFE_ERR_INVALID;
+  const cufe::Batch &b = h->b;
+  if (x_off) std::copy(b.x_off.begin(), b.x_off.end(), x_off);
+  if (chunks) *chunks = (int)b.chunks.size();
+  if (key_bytes) *key_bytes = b.key_bytes;
+  if (scratch_bytes) *scratch_bytes = b.scratch_bytes;
+  return CUFE_OK;
+}
+
+int cufe_batch_instance(const cufe_batch *h, int i, const uint32_t **mpk, const uint32_t **msk, const uint32_t **sky,
+                        const uint32_t **ct) {
+  if (!h || i < 0 || i >= h->b.count) return CUFE_ERR_INVALID;
+  const cufe::Batch &b = h->b;
+  int pos = -1;
+  for (int k = 0; k < b.count; ++k)
+    if ((int)b.inst[k].user == i) pos = k;
+  const cufe::InstDev &I = b.inst[pos];
+  if (mpk) *mpk = b.keys + I.mpk;
+  if (msk) *msk = b.keys + I.msk;
+  if (sky) *sky = b.sky + I.sky;
+  if (ct) *ct = (b.chunks.size() == 1 && b.ran)
+                    ? reinterpret_cast<const uint32_t *>(b.scratch + b.a_ct) + I.ct
+                    : nullptr;
+  return CUFE_OK;
+}
+
+}  // extern "C"

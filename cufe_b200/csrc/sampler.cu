@@ -626,6 +626,40 @@ void aes_sbox(uint8_t out[256]) {
   }
 }
 
+// AES-256 key expansion (FIPS-197 5.2) on the device, one key per thread, into the
+// big-endian round-key words of aes_key_expand: rk[i][60] from seeds[perm ? perm[i] : i][32]
+__global__ void k_expand_keys(const uint8_t *__restrict__ seeds, const uint32_t *__restrict__ perm, uint32_t count,
+                              uint32_t *__restrict__ rk) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint8_t *k = seeds + 32 * (size_t)(perm ? perm[i] : i);
+  uint32_t w[60];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    w[j] = ((uint32_t)k[4 * j] << 24) | ((uint32_t)k[4 * j + 1] << 16) | ((uint32_t)k[4 * j + 2] << 8) | k[4 * j + 3];
+#pragma unroll
+  for (int j = 8; j < 60; ++j) {
+    uint32_t t = w[j - 1];
+    if (j % 8 == 0) t = (t << 8) | (t >> 24);
+    if (j % 8 == 0 || j % 8 == 4)
+      t = ((uint32_t)c_sbox[t >> 24] << 24) | ((uint32_t)c_sbox[(t >> 16) & 255] << 16) |
+          ((uint32_t)c_sbox[(t >> 8) & 255] << 8) | c_sbox[t & 255];
+    if (j % 8 == 0) t ^= (1u << (j / 8 - 1)) << 24;  // round constants 1, 2, 4, ..., 64
+    w[j] = w[j - 8] ^ t;
+  }
+  uint32_t *o = rk + (size_t)i * 60;
+#pragma unroll
+  for (int j = 0; j < 60; ++j) o[j] = w[j];
+}
+
+int expand_keys_device(const uint8_t *d_seeds, const uint32_t *d_perm, uint32_t count, uint32_t *d_rk,
+                       cudaStream_t s) {
+  if (!count) return CUFE_OK;
+  k_expand_keys<<<(count + 127) / 128, 128, 0, s>>>(d_seeds, d_perm, count, d_rk);
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
 int sampler_init_device() {
   uint8_t sbox[256];
   aes_sbox(sbox);

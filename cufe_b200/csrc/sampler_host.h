@@ -15,6 +15,9 @@ void aes_sbox(uint8_t out[256]);
 void aes_key_expand(const uint8_t key[32], uint32_t w[60]);
 
 int sampler_init_device();
+// device key expansion: d_rk[i][60] = aes_key_expand(d_seeds[d_perm ? d_perm[i] : i])
+int expand_keys_device(const uint8_t *d_seeds, const uint32_t *d_perm, uint32_t count, uint32_t *d_rk,
+                       cudaStream_t s);
 
 // CPU stream mapping: nstreams independent AES-CTR streams (round keys d_rkeys[nstreams][60],
 // nonce 0, counter 0), each running `calls` consecutive sampler calls of n samples with

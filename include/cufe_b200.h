@@ -161,6 +161,47 @@ int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0
 int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void *stream);
 
 /* =====================================================================================
+ * 2b. Heterogeneous batches: many independent instances, each with its own ring degree n_i,
+ *     vector length l_i (hence its own p_i = 64 l_i + 1 and floor(q / p_i), src/params.h:26-27)
+ *     and master key pair.  No counterpart in the reference, which runs one instance of
+ *     compile-time size per process; every step below is the reference's algorithm per
+ *     instance (setup src/rlwe_sife.c:32-82, encrypt 112-181, keygen 215-245, decrypt and
+ *     decode of coefficient 0 248-332, CPU stream mapping for all randomness).
+ * ===================================================================================== */
+
+typedef struct cufe_batch cufe_batch;
+
+/* count instances, n[i] a power of two in [256, 8192], l[i] in [1, 4096].  Keys of all
+ * instances stay resident (sum of (2 l_i + 1) * 3 * n_i words); a step processes instances in
+ * chunks whose scratch stays below max_chunk_bytes (0: 24 GiB). */
+int cufe_batch_create(cufe_batch **batch, int count, const int *n, const int *l, size_t max_chunk_bytes, int device);
+int cufe_batch_destroy(cufe_batch *batch);
+/* master keys of every instance from host seeds [count][32] (seeds_s may be NULL: the
+ * reference's zero-key secret stream) */
+int cufe_batch_setup(cufe_batch *batch, const uint8_t *seeds_a, const uint8_t *seeds_s, const uint8_t *seeds_e,
+                     void *stream);
+/* device buffers of a step: d_x (uint32) and d_y (int32, signed) packed by instance, instance i
+ * at word x_off[i] (cufe_batch_info); d_seeds2 / d_seeds3 [count][32] encryption seeds;
+ * d_out[count] the decoded coefficient 0 of d_y in [0, p_i] (the inner product mod p_i);
+ * d_d0 (optional) [count][3] its residues.  Rebinding different buffers drops the graph. */
+int cufe_batch_bind(cufe_batch *batch, const uint32_t *d_x, const int32_t *d_y, const uint8_t *d_seeds2,
+                    const uint8_t *d_seeds3, uint32_t *d_out, uint32_t *d_d0);
+/* one step with the bound buffers, eagerly on `stream` */
+int cufe_batch_run(cufe_batch *batch, void *stream);
+/* the same step from a CUDA graph, captured on the first call (after one eager step, made by
+ * that call if none ran) and replayed afterwards: the graph reads the bound buffers' current
+ * contents, so new seeds or inputs written there take effect on the next replay */
+int cufe_batch_replay(cufe_batch *batch, void *stream);
+/* synchronous check of the batch's sampler status word (CUFE_ERR_SAMPLER if set) */
+int cufe_batch_status(cufe_batch *batch);
+/* x_off[count + 1] (may be NULL), number of chunks, resident key bytes, scratch bytes */
+int cufe_batch_info(const cufe_batch *batch, uint64_t *x_off, int *chunks, size_t *key_bytes, size_t *scratch_bytes);
+/* device addresses of instance i's mpk [(l+1)][3][n], msk [l][3][n], function key [3][n] of
+ * the last step, and (one-chunk batches after a step, else NULL) its ciphertext [(l+1)][3][n] */
+int cufe_batch_instance(const cufe_batch *batch, int i, const uint32_t **mpk, const uint32_t **msk,
+                        const uint32_t **sky, const uint32_t **ct);
+
+/* =====================================================================================
  * 3. Negacyclic NTT on an RNS ring (CT_forward / GS_reverse, src/ntt.c:38-114)
  * ===================================================================================== */
 
