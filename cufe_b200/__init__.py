@@ -81,6 +81,18 @@ def lib():
             "cufe_batch_status": [vp],
             "cufe_batch_info": [vp, vp, vp, vp, vp],
             "cufe_batch_instance": [vp, i, vp, vp, vp, vp],
+            "cufe_server_create": [C.POINTER(vp), i, vp, vp, C.c_size_t, C.c_size_t, i],
+            "cufe_server_destroy": [vp],
+            "cufe_server_setup": [vp, vp, vp, vp],
+            "cufe_server_encrypt": [vp, i, vp, vp, vp, C.c_double],
+            "cufe_server_keygen": [vp, i, vp, C.c_double],
+            "cufe_server_decrypt": [vp, ll, ll, C.c_double],
+            "cufe_server_poll": [vp, i],
+            "cufe_server_pending": [vp, vp, vp],
+            "cufe_server_result": [vp, ll, vp, vp, vp, vp],
+            "cufe_server_read": [vp, ll, vp, C.c_size_t],
+            "cufe_server_release": [vp, ll],
+            "cufe_server_stats": [vp, vp, vp, vp],
             "cufe_ring_set_variant": [vp, i, i],
             "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
@@ -96,6 +108,10 @@ def lib():
             f.argtypes = args
             f.restype = None if name.startswith("rlwe_sife_") else C.c_int
         L.cufe_sampler_refills.restype = C.c_longlong
+        for name in ("cufe_server_encrypt", "cufe_server_keygen", "cufe_server_decrypt"):
+            getattr(L, name).restype = C.c_longlong
+        L.cufe_server_now.argtypes = []
+        L.cufe_server_now.restype = C.c_double
         _lib = L
     return _lib
 
@@ -451,3 +467,93 @@ class Batch:
         t = torch.as_tensor(_View(), device=self.dev)
         torch.cuda.synchronize(self.dev)
         return t.cpu().numpy().view(np.uint32)
+
+
+class Server:
+    """Request server over resident tenants (continuous batching): submit encrypt / keygen /
+    decrypt requests, poll() to make progress, read results by request id."""
+
+    QUEUED, RUNNING, DONE, RELEASED = 0, 1, 2, 3
+
+    def __init__(self, n, l, arena_bytes=0, tick_bytes=0, device=0):
+        self.n = np.ascontiguousarray(n, np.int32)
+        self.l = np.ascontiguousarray(l, np.int32)
+        self.device = device
+        h = C.c_void_p()
+        _check(lib().cufe_server_create(C.byref(h), len(self.n), self.n.ctypes.data, self.l.ctypes.data,
+                                        arena_bytes, tick_bytes, device), "cufe_server_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cufe_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def now():
+        return lib().cufe_server_now()
+
+    def setup(self, seeds_a, seeds_s, seeds_e):
+        a, s_, e = _seeds(seeds_a), _seeds(seeds_s), _seeds(seeds_e)
+        _check(lib().cufe_server_setup(self.h, _ptr(a), _ptr(s_), _ptr(e)), "cufe_server_setup")
+
+    def _id(self, r, what):
+        if r < 0:
+            raise CufeError(int(r), what)
+        return int(r)
+
+    def encrypt(self, tenant, x, seed2, seed3, t_arrival=-1.0):
+        x = np.ascontiguousarray(x, np.uint32)
+        s2, s3 = _seeds(seed2), _seeds(seed3)
+        return self._id(lib().cufe_server_encrypt(self.h, tenant, x.ctypes.data, s2.ctypes.data, s3.ctypes.data,
+                                                  t_arrival), "cufe_server_encrypt")
+
+    def keygen(self, tenant, y, t_arrival=-1.0):
+        y = np.ascontiguousarray(y, np.int32)
+        return self._id(lib().cufe_server_keygen(self.h, tenant, y.ctypes.data, t_arrival), "cufe_server_keygen")
+
+    def decrypt(self, ct, sk, t_arrival=-1.0):
+        return self._id(lib().cufe_server_decrypt(self.h, ct, sk, t_arrival), "cufe_server_decrypt")
+
+    def poll(self, wait=False):
+        r = lib().cufe_server_poll(self.h, int(wait))
+        if r < 0:
+            raise CufeError(r, "cufe_server_poll")
+        return r
+
+    def pending(self):
+        q, t = C.c_longlong(0), C.c_int(0)
+        _check(lib().cufe_server_pending(self.h, C.byref(q), C.byref(t)), "cufe_server_pending")
+        return q.value, t.value
+
+    def drain(self):
+        while True:
+            q, t = self.pending()
+            if q == 0 and t == 0:
+                return
+            self.poll(wait=t > 0)
+
+    def result(self, rid):
+        st, v, ta, td = C.c_int(0), C.c_uint32(0), C.c_double(0), C.c_double(0)
+        _check(lib().cufe_server_result(self.h, rid, C.byref(st), C.byref(v), C.byref(ta), C.byref(td)),
+               "cufe_server_result")
+        return st.value, v.value, ta.value, td.value
+
+    def read(self, rid, words):
+        out = np.zeros(words, np.uint32)
+        _check(lib().cufe_server_read(self.h, rid, out.ctypes.data, words), "cufe_server_read")
+        return out
+
+    def release(self, rid):
+        _check(lib().cufe_server_release(self.h, rid), "cufe_server_release")
+
+    def stats(self):
+        t, d, f = C.c_longlong(0), C.c_longlong(0), C.c_size_t(0)
+        _check(lib().cufe_server_stats(self.h, C.byref(t), C.byref(d), C.byref(f)), "cufe_server_stats")
+        return {"ticks": t.value, "done": d.value, "ct_free_bytes": f.value}

@@ -22,7 +22,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -205,6 +207,8 @@ struct Batch {
   int device = 0, count = 0, num_sms = 148;
   std::vector<int> n, l;         // caller order
   std::vector<uint32_t> order;   // internal position -> caller index
+  std::vector<int> pos_of;       // caller index -> internal position
+  bool keys_only = false;        // hold keys only (no step scratch): the request server's tenants
   std::vector<uint64_t> x_off;   // caller order, count + 1
   std::map<int, std::unique_ptr<Ctx>> ctx;  // one context (ring, setup workspace) per n
   std::vector<BatchChunk> chunks;
@@ -295,6 +299,8 @@ int Batch::create(int count_, const int *n_, const int *l_, size_t max_chunk_byt
   order.resize(count);
   std::iota(order.begin(), order.end(), 0u);
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return n[a] < n[b]; });
+  pos_of.assign(count, 0);
+  for (int pos = 0; pos < count; ++pos) pos_of[order[pos]] = pos;
   // key arena: mpk_i [(l+1)][3][n], msk_i [l][3][n]; function keys [3][n]
   inst.assign(count, InstDev{});
   uint64_t kw = 0, skw = 0;
@@ -422,7 +428,7 @@ int Batch::create(int count_, const int *n_, const int *l_, size_t max_chunk_byt
   CUFE_CUDA(cudaMalloc(&sky, std::max<size_t>(skw * 4, 256)));
   CUFE_CUDA(cudaMalloc(&tables, std::max<size_t>(blob.size(), 256)));
   CUFE_CUDA(cudaMemcpy(tables, blob.data(), blob.size(), cudaMemcpyHostToDevice));
-  CUFE_CUDA(cudaMalloc(&scratch, scratch_bytes));
+  if (!keys_only) CUFE_CUDA(cudaMalloc(&scratch, scratch_bytes));
   CUFE_CUDA(cudaMalloc(&rk, (size_t)2 * count * 60 * 4));
   CUFE_CUDA(cudaMalloc(&perm, (size_t)count * 4));
   CUFE_CUDA(cudaMemcpy(perm, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice));
@@ -568,6 +574,471 @@ int Batch::replay(cudaStream_t s) {
   return CUFE_OK;
 }
 
+
+// ---------------------------------------------------------------------------- serving
+//
+// A request server over resident tenants (a Batch holds their key pairs).  Requests:
+// encrypt(tenant, x, seeds) -> a ciphertext kept in the ciphertext arena; keygen(tenant, y)
+// -> a function key (and its y) kept in the key arena; decrypt(ciphertext, function key) ->
+// the decoded inner product.  poll() retires finished ticks and launches the next: a tick
+// admits queued requests in arrival order while its scratch, the arenas and the table
+// buffer have room (admission by device-memory footprint), uploads one table blob, and runs
+// encrypt (segmented sigma_2 / sigma_3 samplers, r^ NTT, per-degree encryption), keygen and
+// decrypt kernels over all admitted requests.  Requests arriving while ticks run join the
+// next tick; up to two ticks are in flight (one running, one queued behind it).
+
+class WordArena {  // first-fit allocator over [0, words)
+ public:
+  void init(uint64_t words) {
+    free_.clear();
+    if (words) free_[0] = words;
+    total_ = avail_ = words;
+  }
+  bool alloc(uint64_t w, uint64_t *off) {
+    w = (w + 63) & ~63ull;  // 256-byte granules
+    for (auto it = free_.begin(); it != free_.end(); ++it)
+      if (it->second >= w) {
+        *off = it->first;
+        const uint64_t rest = it->second - w, at = it->first + w;
+        free_.erase(it);
+        if (rest) free_[at] = rest;
+        avail_ -= w;
+        return true;
+      }
+    return false;
+  }
+  void release(uint64_t off, uint64_t w) {
+    w = (w + 63) & ~63ull;
+    auto it = free_.emplace(off, w).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+    avail_ += w;
+  }
+  uint64_t available() const { return avail_; }
+
+ private:
+  std::map<uint64_t, uint64_t> free_;
+  uint64_t total_ = 0, avail_ = 0;
+};
+
+enum { REQ_ENCRYPT = 0, REQ_KEYGEN = 1, REQ_DECRYPT = 2 };
+enum { ST_QUEUED = 0, ST_RUNNING = 1, ST_DONE = 2, ST_RELEASED = 3 };
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Server {
+  struct Req {
+    int kind = 0, tenant = 0, state = ST_QUEUED;
+    std::vector<uint32_t> data;  // x (encrypt) or the bits of y (keygen)
+    uint8_t s2[32], s3[32];
+    int64_t ref_ct = -1, ref_sk = -1;
+    uint64_t slot = 0, slot_words = 0;  // ciphertext / function-key slot
+    int refs = 0;                       // decrypts not yet finished that read this slot
+    bool release_pending = false;
+    uint32_t value = 0;
+    double t_arrival = 0, t_done = 0;
+  };
+  struct Tick {
+    cudaEvent_t done = nullptr;
+    std::vector<int64_t> ids, dec_ids;
+    uint8_t *stage = nullptr;  // pinned: table blob, then the y vectors of keygens
+    uint32_t *host_out = nullptr;
+    bool busy = false;
+  };
+
+  Batch tenants;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<Req> reqs;
+  std::deque<int64_t> queue;
+  std::deque<int> inflight;  // tick indices in launch order
+  Tick ticks[2];
+  WordArena ct_arena, sk_arena;
+  uint32_t *d_ct = nullptr, *d_sk = nullptr, *d_out = nullptr;
+  uint8_t *d_tab = nullptr, *d_scr = nullptr;
+  size_t tab_bytes = 0, scr_bytes = 0;
+  static constexpr int kMaxDec = 65536;
+  static constexpr size_t kStageY = (size_t)32 << 20;  // pinned room for a tick's keygen vectors
+  uint64_t n_ticks = 0, n_done = 0;
+
+  int create(int count, const int *n, const int *l, size_t arena_bytes, size_t tick_bytes, int dev) {
+    device = dev;
+    tenants.keys_only = true;  // the tenants' key pairs; ticks use the server's own scratch
+    int rc = tenants.create(count, n, l, (size_t)1 << 40, dev);
+    if (rc) return rc;
+    if (!arena_bytes) arena_bytes = (size_t)16 << 30;
+    if (!tick_bytes) tick_bytes = (size_t)16 << 30;
+    tab_bytes = (size_t)64 << 20;
+    scr_bytes = tick_bytes;
+    CUFE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CUFE_CUDA(cudaMalloc(&d_ct, arena_bytes));
+    CUFE_CUDA(cudaMalloc(&d_sk, arena_bytes / 4));
+    CUFE_CUDA(cudaMalloc(&d_out, (size_t)kMaxDec * 4));
+    CUFE_CUDA(cudaMalloc(&d_tab, tab_bytes));
+    CUFE_CUDA(cudaMalloc(&d_scr, scr_bytes));
+    ct_arena.init(arena_bytes / 4);
+    sk_arena.init(arena_bytes / 16);
+    for (Tick &t : ticks) {
+      CUFE_CUDA(cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming));
+      CUFE_CUDA(cudaMallocHost(&t.stage, tab_bytes + kStageY));
+      CUFE_CUDA(cudaMallocHost(&t.host_out, (size_t)kMaxDec * 4));
+    }
+    return CUFE_OK;
+  }
+
+  void release_all() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (Tick &t : ticks) {
+      if (t.done) cudaEventDestroy(t.done);
+      if (t.stage) cudaFreeHost(t.stage);
+      if (t.host_out) cudaFreeHost(t.host_out);
+      t = Tick{};
+    }
+    for (void *p : {(void *)d_ct, (void *)d_sk, (void *)d_out, (void *)d_tab, (void *)d_scr})
+      if (p) cudaFree(p);
+    d_ct = d_sk = d_out = nullptr;
+    d_tab = d_scr = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    tenants.release();
+  }
+
+  const InstDev &tenant(int t) const { return tenants.inst[tenants.pos_of[t]]; }
+
+  int64_t submit(Req &&r) {
+    reqs.push_back(std::move(r));
+    const int64_t id = (int64_t)reqs.size() - 1;
+    Req &q = reqs.back();
+    if (q.kind == REQ_DECRYPT) {
+      ++reqs[q.ref_ct].refs;
+      ++reqs[q.ref_sk].refs;
+    }
+    queue.push_back(id);
+    return id;
+  }
+
+  static uint64_t enc_scratch_bytes(uint32_t n, uint32_t l) {
+    const uint64_t poly = (uint64_t)3 * n * 4;
+    const uint64_t R3 = cpu_map_refills(l, n, 2), R2 = cpu_map_refills(2, n, 1);
+    return poly * (2 + 2 + l) + std::max(R3, R2) * 70 + 2 * 60 * 4 + 8192;
+  }
+
+  void retire(Tick &t) {
+    const double now = now_s();
+    for (size_t k = 0; k < t.dec_ids.size(); ++k) reqs[t.dec_ids[k]].value = t.host_out[k];
+    for (int64_t id : t.ids) {
+      Req &r = reqs[id];
+      r.state = ST_DONE;
+      r.t_done = now;
+      ++n_done;
+      if (r.kind == REQ_DECRYPT) {
+        for (int64_t ref : {r.ref_ct, r.ref_sk}) {
+          Req &o = reqs[ref];
+          if (--o.refs == 0 && o.release_pending) free_slot(o);
+        }
+      }
+    }
+    t.ids.clear();
+    t.dec_ids.clear();
+    t.busy = false;
+  }
+
+  void free_slot(Req &o) {
+    if (o.state == ST_RELEASED) return;
+    if (o.kind == REQ_ENCRYPT) ct_arena.release(o.slot, o.slot_words);
+    if (o.kind == REQ_KEYGEN) sk_arena.release(o.slot, o.slot_words);
+    o.state = ST_RELEASED;
+  }
+
+  // retire finished ticks; launch one if a tick buffer is free and work is queued
+  int poll(bool wait) {
+    int done0 = (int)n_done;
+    while (!inflight.empty()) {
+      Tick &t = ticks[inflight.front()];
+      cudaError_t e = wait ? cudaEventSynchronize(t.done) : cudaEventQuery(t.done);
+      if (e == cudaErrorNotReady) break;
+      if (e != cudaSuccess) {
+        set_last_error(std::string("server tick: ") + cudaGetErrorString(e));
+        return CUFE_ERR_CUDA;
+      }
+      retire(t);
+      inflight.pop_front();
+      wait = false;
+    }
+    if (!queue.empty() && inflight.size() < 2) {
+      const int ti = ticks[0].busy ? 1 : 0;
+      int rc = launch(ti);
+      if (rc) return rc;
+    }
+    return (int)n_done - done0;
+  }
+
+  int launch(int ti) {
+    Tick &T = ticks[ti];
+    // ---- admission (arrival order; a decrypt waits until its inputs were admitted)
+    std::vector<int64_t> enc, kg, dec;
+    uint64_t scr = 0, x_words = 0, blob_est = 1 << 16, ystage = 0;
+    std::deque<int64_t> keep;
+    const uint64_t scr_cap = scr_bytes - (1u << 20);
+    while (!queue.empty()) {
+      const int64_t id = queue.front();
+      queue.pop_front();
+      Req &r = reqs[id];
+      const InstDev &I = tenant(r.tenant);
+      bool ok = true;
+      if (r.kind == REQ_ENCRYPT) {
+        const uint64_t need = enc_scratch_bytes(I.n, I.l), tab = 2 * sizeof(InstDev) + 512 + 4ull * I.l;
+        ok = scr + need <= scr_cap && blob_est + tab <= tab_bytes && enc.size() < 4096 &&
+             ct_arena.alloc((uint64_t)(I.l + 1) * 3 * I.n, &r.slot);
+        if (ok) {
+          r.slot_words = (uint64_t)(I.l + 1) * 3 * I.n;
+          scr += need;
+          blob_est += tab;
+          x_words += I.l;
+          enc.push_back(id);
+        }
+      } else if (r.kind == REQ_KEYGEN) {
+        const uint64_t yb = a256(4ull * I.l);
+        ok = kg.size() < 4096 && ystage + yb <= kStageY && blob_est + 2 * sizeof(InstDev) <= tab_bytes &&
+             sk_arena.alloc((uint64_t)3 * I.n + I.l, &r.slot);
+        if (ok) {
+          r.slot_words = (uint64_t)3 * I.n + I.l;
+          ystage += yb;
+          blob_est += 2 * sizeof(InstDev);
+          kg.push_back(id);
+        }
+      } else {
+        ok = dec.size() < (size_t)kMaxDec && blob_est + sizeof(InstDev) <= tab_bytes &&
+             reqs[r.ref_ct].state != ST_QUEUED && reqs[r.ref_sk].state != ST_QUEUED;
+        if (ok) {
+          blob_est += sizeof(InstDev);
+          dec.push_back(id);
+        }
+      }
+      if (ok) {
+        r.state = ST_RUNNING;
+      } else {
+        keep.push_back(id);
+        if (r.kind == REQ_ENCRYPT && scr + enc_scratch_bytes(I.n, I.l) > scr_cap) break;  // tick full
+      }
+    }
+    while (!keep.empty()) {
+      queue.push_front(keep.back());
+      keep.pop_back();
+    }
+    if (enc.empty() && kg.empty() && dec.empty()) return CUFE_OK;
+    // ---- tables: encryptions grouped by ring degree
+    std::stable_sort(enc.begin(), enc.end(),
+                     [&](int64_t a, int64_t b) { return tenant(reqs[a].tenant).n < tenant(reqs[b].tenant).n; });
+    std::vector<uint8_t> blob;
+    auto put = [&](const void *src, size_t bytes) {
+      const size_t off = a256(blob.size());
+      blob.resize(off + a256(bytes));
+      if (src && bytes) std::memcpy(blob.data() + off, src, bytes);
+      return off;
+    };
+    const uint32_t ne = (uint32_t)enc.size();
+    std::vector<InstDev> ei(ne);
+    std::vector<uint32_t> calls2(ne, 2), nn(ne), calls3(ne);
+    std::vector<uint64_t> o2(ne), o3(ne);
+    uint64_t w_s2o = 0, w_rh = 0, w_f3 = 0, w_x = 0;
+    std::vector<BatchGroup> groups;
+    std::vector<uint32_t> xs;
+    xs.reserve(x_words);
+    for (uint32_t k = 0; k < ne; ++k) {
+      const Req &r = reqs[enc[k]];
+      InstDev I = tenant(r.tenant);
+      const int logn = __builtin_ctz(I.n);
+      if (groups.empty() || groups.back().logn != logn) {
+        BatchGroup g;
+        g.logn = logn;
+        g.first = k;
+        g.rh = w_rh;
+        g.s2o = w_s2o;
+        groups.push_back(g);
+      }
+      ++groups.back().count;
+      groups.back().nres += (long long)(I.l + 1) * 3;
+      I.ct = r.slot;
+      I.s2o = w_s2o;
+      I.rh = w_rh;
+      I.f3 = w_f3;
+      I.x = w_x;
+      xs.insert(xs.end(), r.data.begin(), r.data.end());
+      nn[k] = I.n;
+      calls3[k] = I.l;
+      o2[k] = w_s2o;
+      o3[k] = w_f3;
+      w_s2o += (uint64_t)6 * I.n;
+      w_rh += (uint64_t)3 * I.n;
+      w_f3 += (uint64_t)I.l * 3 * I.n;
+      w_x += I.l;
+      ei[k] = I;
+    }
+    SegSizes z2{}, z3{};
+    size_t seg2 = 0, seg3 = 0, x_off = 0, seeds_off = 0;
+    for (BatchGroup &g : groups) {
+      g.inst_off = put(ei.data() + g.first, (size_t)g.count * sizeof(InstDev));
+      std::vector<uint64_t> ro(g.count + 1, 0);
+      for (uint32_t k = 0; k < g.count; ++k) ro[k + 1] = ro[k] + (uint64_t)(ei[g.first + k].l + 1) * 3;
+      g.res_off = put(ro.data(), ro.size() * 8);
+    }
+    if (ne) {
+      std::vector<uint8_t> t2(seg_layout(ne).bytes), t3(seg_layout(ne).bytes);
+      z2 = seg_fill_host(1, ne, calls2.data(), nn.data(), o2.data(), t2.data());
+      z3 = seg_fill_host(2, ne, calls3.data(), nn.data(), o3.data(), t3.data());
+      seg2 = put(t2.data(), t2.size());
+      seg3 = put(t3.data(), t3.size());
+      x_off = put(xs.data(), xs.size() * 4);
+      std::vector<uint8_t> sd((size_t)2 * ne * 32);
+      for (uint32_t k = 0; k < ne; ++k) {
+        std::memcpy(sd.data() + 32 * (size_t)k, reqs[enc[k]].s2, 32);
+        std::memcpy(sd.data() + 32 * (size_t)(ne + k), reqs[enc[k]].s3, 32);
+      }
+      seeds_off = put(sd.data(), sd.size());
+    }
+    // keygen: y lives in the function-key slot after its 3n words
+    std::vector<InstDev> ki(kg.size());
+    std::vector<uint64_t> uo(kg.size() + 1, 0);
+    for (size_t k = 0; k < kg.size(); ++k) {
+      const Req &r = reqs[kg[k]];
+      InstDev I = tenant(r.tenant);
+      I.sky = r.slot;
+      I.x = r.slot + (uint64_t)3 * I.n;
+      ki[k] = I;
+      uo[k + 1] = uo[k] + (uint64_t)3 * I.n / 256;
+    }
+    uint32_t max_l = 1;
+    for (const InstDev &I : ki) max_l = std::max(max_l, I.l);
+    const size_t kg_inst = put(ki.data(), ki.size() * sizeof(InstDev)), kg_units = put(uo.data(), uo.size() * 8);
+    // decrypt: ciphertext slot, function-key slot and its y
+    std::vector<InstDev> di(dec.size());
+    for (size_t k = 0; k < dec.size(); ++k) {
+      const Req &r = reqs[dec[k]];
+      const Req &c = reqs[r.ref_ct], &f = reqs[r.ref_sk];
+      InstDev I = tenant(c.tenant);
+      I.ct = c.slot;
+      I.sky = f.slot;
+      I.x = f.slot + (uint64_t)3 * I.n;
+      I.user = (uint32_t)k;
+      di[k] = I;
+    }
+    const size_t dec_inst = put(di.data(), di.size() * sizeof(InstDev));
+    if (blob.size() > tab_bytes) {  // cannot happen with the admission limits; refuse loudly
+      set_last_error("server: tick tables exceed the table buffer");
+      return CUFE_ERR_INVALID;
+    }
+    // ---- upload and launch (all on the server stream)
+    std::memcpy(T.stage, blob.data(), blob.size());
+    CUFE_CUDA(cudaMemcpyAsync(d_tab, T.stage, blob.size(), cudaMemcpyHostToDevice, stream));
+    size_t ys = a256(blob.size());
+    for (size_t k = 0; k < kg.size(); ++k) {
+      const Req &r = reqs[kg[k]];
+      std::memcpy(T.stage + ys, r.data.data(), r.data.size() * 4);
+      CUFE_CUDA(cudaMemcpyAsync(d_sk + ki[k].x, T.stage + ys, r.data.size() * 4, cudaMemcpyHostToDevice, stream));
+      ys += a256(r.data.size() * 4);
+    }
+    int rc = CUFE_OK;
+    if (ne) {
+      // scratch: s2o | rh | rh_sh | f3 | round keys | sampler scratch
+      uint8_t *p = d_scr;
+      auto take = [&](size_t b) {
+        uint8_t *q = p;
+        p += a256(b);
+        return q;
+      };
+      uint32_t *s2o = reinterpret_cast<uint32_t *>(take(w_s2o * 4));
+      uint32_t *rh = reinterpret_cast<uint32_t *>(take(w_rh * 4));
+      uint32_t *rhsh = reinterpret_cast<uint32_t *>(take(w_rh * 4));
+      uint32_t *f3 = reinterpret_cast<uint32_t *>(take(w_f3 * 4));
+      uint32_t *rk = reinterpret_cast<uint32_t *>(take((size_t)2 * ne * 60 * 4));
+      void *samp = take(std::max(seg_scratch_bytes(z2), seg_scratch_bytes(z3)));
+      if ((size_t)(p - d_scr) > scr_bytes) {
+        set_last_error("server: tick scratch exceeded");
+        return CUFE_ERR_INVALID;
+      }
+      const uint8_t *seeds = d_tab + seeds_off;
+      if ((rc = expand_keys_device(seeds, nullptr, 2 * ne, rk, stream))) return rc;
+      if ((rc = sample_cpu_map_seg(1, seg_bind(d_tab + seg2, ne), z2, rk, s2o, samp, tenants.status, tenants.num_sms,
+                                   stream, nullptr)))
+        return rc;
+      for (const BatchGroup &g : groups) {
+        const size_t nn1 = (size_t)1 << g.logn;
+        CUFE_CUDA(cudaMemcpy2DAsync(rh + g.rh, 3 * nn1 * 4, s2o + g.s2o, 6 * nn1 * 4, 3 * nn1 * 4, g.count,
+                                    cudaMemcpyDeviceToDevice, stream));
+        if ((rc = ntt_fwd_shoup_launch(tenants.ctx[(int)nn1]->ring.args, rh + g.rh, rhsh + g.rh,
+                                       (long long)g.count * 3, stream)))
+          return rc;
+      }
+      if ((rc = sample_cpu_map_seg(2, seg_bind(d_tab + seg3, ne), z3, rk + (size_t)ne * 60, f3, samp, tenants.status,
+                                   tenants.num_sms, stream, nullptr)))
+        return rc;
+      const uint32_t *xd = reinterpret_cast<const uint32_t *>(d_tab + x_off);
+      for (const BatchGroup &g : groups) {
+        const RingArgs &ra = tenants.ctx[1 << g.logn]->ring.args;
+        rc = dispatch_logn_b(g.logn, [&](auto LL) {
+          constexpr int LOGN = decltype(LL)::value;
+          using P = NttPlan<LOGN>;
+          constexpr int G = ppc<LOGN>();
+          static bool attr = false;
+          if (!attr) {
+            CUFE_CUDA(cudaFuncSetAttribute(k_encrypt_het<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+            attr = true;
+          }
+          ProfScope ps("serve_encrypt", stream);
+          k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, stream>>>(
+              reinterpret_cast<const InstDev *>(d_tab + g.inst_off), reinterpret_cast<const uint64_t *>(d_tab + g.res_off),
+              g.count, g.nres, tenants.keys, rh, rhsh, f3, s2o, xd, d_ct, ra, tenants.mq);
+          CUFE_CUDA(cudaGetLastError());
+          return (int)CUFE_OK;
+        });
+        if (rc) return rc;
+      }
+    }
+    if (!kg.empty()) {
+      static bool attr = false;
+      if (!attr) {
+        CUFE_CUDA(cudaFuncSetAttribute(k_keygen_het, cudaFuncAttributeMaxDynamicSharedMemorySize, 32 * 1024));
+        attr = true;
+      }
+      ProfScope ps("serve_keygen", stream);
+      k_keygen_het<<<(unsigned)uo.back(), 256, (size_t)2 * max_l * 4, stream>>>(
+          reinterpret_cast<const InstDev *>(d_tab + kg_inst), reinterpret_cast<const uint64_t *>(d_tab + kg_units),
+          (uint32_t)kg.size(), tenants.keys, reinterpret_cast<const int32_t *>(d_sk), d_sk, tenants.mq);
+      CUFE_CUDA(cudaGetLastError());
+    }
+    if (!dec.empty()) {
+      ProfScope ps("serve_decrypt", stream);
+      k_dec_coef0_het<<<(unsigned)dec.size(), 256, 0, stream>>>(reinterpret_cast<const InstDev *>(d_tab + dec_inst),
+                                                               d_ct, d_sk, reinterpret_cast<const int32_t *>(d_sk),
+                                                               d_out, nullptr, tenants.mq, tenants.dd);
+      CUFE_CUDA(cudaGetLastError());
+      CUFE_CUDA(cudaMemcpyAsync(T.host_out, d_out, dec.size() * 4, cudaMemcpyDeviceToHost, stream));
+    }
+    CUFE_CUDA(cudaEventRecord(T.done, stream));
+    T.ids = enc;
+    T.ids.insert(T.ids.end(), kg.begin(), kg.end());
+    T.ids.insert(T.ids.end(), dec.begin(), dec.end());
+    T.dec_ids = dec;
+    T.busy = true;
+    inflight.push_back((int)(&T - ticks));
+    ++n_ticks;
+    return CUFE_OK;
+  }
+};
+
 }  // namespace cufe
 
 // ---------------------------------------------------------------------------- C ABI
@@ -681,6 +1152,163 @@ int cufe_batch_instance(const cufe_batch *h, int i, const uint32_t **mpk, const 
   if (ct) *ct = (b.chunks.size() == 1 && b.ran)
                     ? reinterpret_cast<const uint32_t *>(b.scratch + b.a_ct) + I.ct
                     : nullptr;
+  return CUFE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- server C ABI
+
+struct cufe_server {
+  cufe::Server s;
+  std::mutex mu;
+};
+
+extern "C" {
+
+double cufe_server_now(void) { return cufe::now_s(); }
+
+int cufe_server_create(cufe_server **out, int tenants, const int *n, const int *l, size_t arena_bytes,
+                       size_t tick_bytes, int device) {
+  if (!out) return CUFE_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cufe::set_last_error("no CUDA device");
+    return CUFE_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return CUFE_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return CUFE_ERR_CUDA;
+  cufe_server *h = new cufe_server;
+  const int rc = h->s.create(tenants, n, l, arena_bytes, tick_bytes, device);
+  if (rc) {
+    h->s.release_all();
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return CUFE_OK;
+}
+
+int cufe_server_destroy(cufe_server *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  cudaSetDevice(h->s.device);
+  h->s.release_all();
+  delete h;
+  return CUFE_OK;
+}
+
+int cufe_server_setup(cufe_server *h, const uint8_t *seeds_a, const uint8_t *seeds_s, const uint8_t *seeds_e) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->s.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  int rc = h->s.tenants.setup(seeds_a, seeds_s, seeds_e, h->s.stream);
+  if (rc) return rc;
+  CUFE_CUDA(cudaStreamSynchronize(h->s.stream));
+  return CUFE_OK;
+}
+
+long long cufe_server_encrypt(cufe_server *h, int tenant, const uint32_t *x, const uint8_t *seed2,
+                              const uint8_t *seed3, double t_arrival) {
+  if (!h || !x || !seed2 || !seed3 || tenant < 0 || tenant >= h->s.tenants.count) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  cufe::Server::Req r;
+  r.kind = cufe::REQ_ENCRYPT;
+  r.tenant = tenant;
+  r.data.assign(x, x + h->s.tenants.l[tenant]);
+  std::memcpy(r.s2, seed2, 32);
+  std::memcpy(r.s3, seed3, 32);
+  r.t_arrival = t_arrival >= 0 ? t_arrival : cufe::now_s();
+  return h->s.submit(std::move(r));
+}
+
+long long cufe_server_keygen(cufe_server *h, int tenant, const int32_t *y, double t_arrival) {
+  if (!h || !y || tenant < 0 || tenant >= h->s.tenants.count) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  cufe::Server::Req r;
+  r.kind = cufe::REQ_KEYGEN;
+  r.tenant = tenant;
+  r.data.assign(reinterpret_cast<const uint32_t *>(y), reinterpret_cast<const uint32_t *>(y) + h->s.tenants.l[tenant]);
+  r.t_arrival = t_arrival >= 0 ? t_arrival : cufe::now_s();
+  return h->s.submit(std::move(r));
+}
+
+long long cufe_server_decrypt(cufe_server *h, long long ct, long long sk, double t_arrival) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  auto &R = h->s.reqs;
+  if (ct < 0 || sk < 0 || ct >= (long long)R.size() || sk >= (long long)R.size() ||
+      R[ct].kind != cufe::REQ_ENCRYPT || R[sk].kind != cufe::REQ_KEYGEN || R[ct].tenant != R[sk].tenant ||
+      R[ct].state == cufe::ST_RELEASED || R[sk].state == cufe::ST_RELEASED || R[ct].release_pending ||
+      R[sk].release_pending) {
+    cufe::set_last_error("decrypt: needs a live ciphertext and function key of the same tenant");
+    return CUFE_ERR_INVALID;
+  }
+  cufe::Server::Req r;
+  r.kind = cufe::REQ_DECRYPT;
+  r.tenant = R[ct].tenant;
+  r.ref_ct = ct;
+  r.ref_sk = sk;
+  r.t_arrival = t_arrival >= 0 ? t_arrival : cufe::now_s();
+  return h->s.submit(std::move(r));
+}
+
+int cufe_server_poll(cufe_server *h, int wait) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->s.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return h->s.poll(wait != 0);
+}
+
+int cufe_server_pending(cufe_server *h, long long *queued, int *ticks_in_flight) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (queued) *queued = (long long)h->s.queue.size();
+  if (ticks_in_flight) *ticks_in_flight = (int)h->s.inflight.size();
+  return CUFE_OK;
+}
+
+int cufe_server_result(cufe_server *h, long long id, int *state, uint32_t *value, double *t_arrival, double *t_done) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (id < 0 || id >= (long long)h->s.reqs.size()) return CUFE_ERR_INVALID;
+  const auto &r = h->s.reqs[id];
+  if (state) *state = r.state;
+  if (value) *value = r.value;
+  if (t_arrival) *t_arrival = r.t_arrival;
+  if (t_done) *t_done = r.t_done;
+  return CUFE_OK;
+}
+
+int cufe_server_read(cufe_server *h, long long id, uint32_t *host, size_t words) {
+  if (!h || !host) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (id < 0 || id >= (long long)h->s.reqs.size()) return CUFE_ERR_INVALID;
+  const auto &r = h->s.reqs[id];
+  if (r.state != cufe::ST_DONE || r.kind == cufe::REQ_DECRYPT || words > r.slot_words) return CUFE_ERR_INVALID;
+  const uint32_t *src = (r.kind == cufe::REQ_ENCRYPT ? h->s.d_ct : h->s.d_sk) + r.slot;
+  if (cudaSetDevice(h->s.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  CUFE_CUDA(cudaMemcpy(host, src, words * 4, cudaMemcpyDeviceToHost));
+  return CUFE_OK;
+}
+
+int cufe_server_release(cufe_server *h, long long id) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (id < 0 || id >= (long long)h->s.reqs.size()) return CUFE_ERR_INVALID;
+  auto &r = h->s.reqs[id];
+  if (r.kind == cufe::REQ_DECRYPT || r.state != cufe::ST_DONE) return CUFE_ERR_INVALID;
+  r.release_pending = true;
+  if (r.refs == 0) h->s.free_slot(r);
+  return CUFE_OK;
+}
+
+int cufe_server_stats(cufe_server *h, long long *ticks, long long *done, size_t *ct_free_bytes) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (ticks) *ticks = (long long)h->s.n_ticks;
+  if (done) *done = (long long)h->s.n_done;
+  if (ct_free_bytes) *ct_free_bytes = (size_t)h->s.ct_arena.available() * 4;
   return CUFE_OK;
 }
 

@@ -202,6 +202,51 @@ int cufe_batch_instance(const cufe_batch *batch, int i, const uint32_t **mpk, co
                         const uint32_t **sky, const uint32_t **ct);
 
 /* =====================================================================================
+ * 2c. Request server over resident tenants (continuous batching).  No counterpart in the
+ *     reference.  Tenants are instances with their own (n, l) and key pair (set up as in
+ *     section 2b).  Requests are queued on submission and served in ticks: cufe_server_poll
+ *     retires finished ticks and launches the next one over every queued request that fits
+ *     (arrival order; admission by device-memory footprint: tick scratch, ciphertext arena,
+ *     function-key arena), with up to two ticks in flight.  Each request computes the
+ *     reference's algorithm on its own inputs only, so its result does not depend on what it
+ *     was batched with.  Calls on one server are serialised by a lock.
+ * ===================================================================================== */
+
+typedef struct cufe_server cufe_server;
+
+/* tenants with n[i] a power of two in [256, 8192] and l[i] in [1, 4096]; arena_bytes for
+ * resident ciphertexts (function keys get a quarter of that), tick_bytes of scratch per tick
+ * (0: 16 GiB each) */
+int cufe_server_create(cufe_server **server, int tenants, const int *n, const int *l, size_t arena_bytes,
+                       size_t tick_bytes, int device);
+int cufe_server_destroy(cufe_server *server);
+/* tenant key pairs from host seeds [tenants][32] (seeds_s may be NULL); synchronous */
+int cufe_server_setup(cufe_server *server, const uint8_t *seeds_a, const uint8_t *seeds_s, const uint8_t *seeds_e);
+/* the server's clock in seconds (steady); request arrival times use it */
+double cufe_server_now(void);
+/* submit a request; host inputs are copied; t_arrival < 0 means now.  Returns a request id
+ * (>= 0) or a negative status.  encrypt: x[l] of the tenant, two 32-byte seeds (CPU stream
+ * mapping); keygen: signed y[l]; decrypt: a ciphertext and a function key (request ids of
+ * the same tenant), result = the decoded coefficient 0 of d_y in [0, p] */
+long long cufe_server_encrypt(cufe_server *server, int tenant, const uint32_t *x, const uint8_t *seed2,
+                              const uint8_t *seed3, double t_arrival);
+long long cufe_server_keygen(cufe_server *server, int tenant, const int32_t *y, double t_arrival);
+long long cufe_server_decrypt(cufe_server *server, long long ciphertext, long long function_key, double t_arrival);
+/* retire finished ticks and launch the next; wait != 0 first blocks on the oldest tick in
+ * flight.  Returns the number of requests completed by this call or a negative status. */
+int cufe_server_poll(cufe_server *server, int wait);
+int cufe_server_pending(cufe_server *server, long long *queued, int *ticks_in_flight);
+/* state: 0 queued, 1 running, 2 done, 3 released; value: a decrypt's result */
+int cufe_server_result(cufe_server *server, long long id, int *state, uint32_t *value, double *t_arrival,
+                       double *t_done);
+/* copy a finished encrypt's ciphertext [(l+1)][3][n] or keygen's function key [3][n] (then
+ * y[l]) to host memory (synchronous) */
+int cufe_server_read(cufe_server *server, long long id, uint32_t *host, size_t words);
+/* free a finished encrypt's or keygen's slot once no queued decrypt reads it */
+int cufe_server_release(cufe_server *server, long long id);
+int cufe_server_stats(cufe_server *server, long long *ticks, long long *done, size_t *ct_free_bytes);
+
+/* =====================================================================================
  * 3. Negacyclic NTT on an RNS ring (CT_forward / GS_reverse, src/ntt.c:38-114)
  * ===================================================================================== */
 
