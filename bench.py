@@ -700,6 +700,139 @@ def batched_mixed(args):
     return 0 if ok else 1
 
 
+def serving(args):
+    """Serving loop: open-loop Poisson arrivals at each rate for `duration` seconds, request mix
+    encrypt:keygen:decrypt = 4:1:4, tenants with l log-uniform in [64, 1024] and N in
+    {2048, 4096} (keys resident), seeded from SplitMix64(0xC0FE0005 + i).  Decryptions read a
+    resident pool of ciphertexts and function keys per tenant (their inner products are
+    checked); new ciphertexts and keys are released as they complete.  Latency = completion
+    seen by the server's poll minus the scheduled arrival time.  The plain form serves a
+    sample of the same requests one per tick, each to completion, on the same kernels."""
+    import cufe_b200 as cf
+    T = args.tenants
+    ns, ls = [], []
+    for i in range(T):
+        r = np.random.default_rng(splitmix64(0xC0FE0005 + i))
+        ls.append(int(round(float(np.exp(r.uniform(np.log(64), np.log(1024)))))))
+        ns.append(2048 if r.random() < 0.5 else 4096)
+    rng = np.random.default_rng(0xC0FE0005)
+    S = cf.Server(ns, ls, arena_bytes=args.arena_gb << 30, tick_bytes=args.tick_gb << 30)
+    S.setup(rng.integers(0, 256, (T, 32), dtype=np.uint8), None, rng.integers(0, 256, (T, 32), dtype=np.uint8))
+    # resident pool: 2 ciphertexts and 2 function keys per tenant
+    pool = []
+    for t in range(T):
+        xs = [rng.integers(0, 5, ls[t]).astype(np.uint32) for _ in range(2)]
+        ys = [rng.integers(-16, 17, ls[t]).astype(np.int32) for _ in range(2)]
+        cts = [S.encrypt(t, x, rng.integers(0, 256, 32, dtype=np.uint8), rng.integers(0, 256, 32, dtype=np.uint8))
+               for x in xs]
+        sks = [S.keygen(t, y) for y in ys]
+        pool.append((xs, ys, cts, sks))
+    S.drain()
+    kinds = np.array([0] * 4 + [1] + [2] * 4)
+
+    def make_requests(k, rate):
+        gaps = rng.exponential(1.0 / rate, k)
+        when = np.cumsum(gaps)
+        reqs = []
+        for i in range(k):
+            kind = int(kinds[rng.integers(0, 9)])
+            t = int(rng.integers(0, T))
+            if kind == 0:
+                reqs.append((when[i], 0, t, rng.integers(0, 5, ls[t]).astype(np.uint32),
+                             rng.integers(0, 256, 32, dtype=np.uint8), rng.integers(0, 256, 32, dtype=np.uint8)))
+            elif kind == 1:
+                reqs.append((when[i], 1, t, rng.integers(-16, 17, ls[t]).astype(np.int32)))
+            else:
+                reqs.append((when[i], 2, t, int(rng.integers(0, 2)), int(rng.integers(0, 2))))
+        return reqs
+
+    def submit(req, t_arr):
+        if req[1] == 0:
+            return S.encrypt(req[2], req[3], req[4], req[5], t_arr)
+        if req[1] == 1:
+            return S.keygen(req[2], req[3], t_arr)
+        xs, ys, cts, sks = pool[req[2]]
+        return S.decrypt(cts[req[3]], sks[req[4]], t_arr)
+
+    def check(req, rid):
+        st, v, ta, td = S.result(rid)
+        ok = st in (S.DONE, S.RELEASED)
+        if req[1] == 2:
+            xs, ys, _, _ = pool[req[2]]
+            p = 64 * ls[req[2]] + 1
+            ok = ok and v % p == int(xs[req[3]].astype(np.int64) @ ys[req[4]].astype(np.int64)) % p
+        return ok, 1000.0 * (td - ta)
+
+    results = []
+    for rate in args.rates:
+        reqs = make_requests(max(1, int(rate * args.duration)), rate)
+        t0 = S.now() + 0.01
+        ids, owned = [], []
+        t_pos = 0
+        t_stat0 = S.stats()
+        while t_pos < len(reqs):
+            now = S.now()
+            while t_pos < len(reqs) and t0 + reqs[t_pos][0] <= now:
+                rid = submit(reqs[t_pos], t0 + reqs[t_pos][0])
+                ids.append(rid)
+                if reqs[t_pos][1] != 2:
+                    owned.append(rid)
+                t_pos += 1
+            S.poll()
+            # release finished ciphertexts / keys (oldest first) to bound the arenas
+            while owned and S.result(owned[0])[0] == S.DONE:
+                S.release(owned.pop(0))
+        while True:
+            q, fl = S.pending()
+            while owned and S.result(owned[0])[0] == S.DONE:
+                S.release(owned.pop(0))
+            if q == 0 and fl == 0:
+                break
+            S.poll(wait=fl > 0)
+        t_end = max(S.result(i)[3] for i in ids)
+        lat = {0: [], 1: [], 2: []}
+        ok = True
+        for req, rid in zip(reqs, ids):
+            good, ms = check(req, rid)
+            ok = ok and good
+            lat[req[1]].append(ms)
+        for rid in owned:
+            S.release(rid)
+        st = S.stats()
+        allv = lat[0] + lat[1] + lat[2]
+        pct = lambda v: {"p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99)),  # noqa: E731
+                         "n": len(v)} if v else None
+        results.append({"rate_rps": rate, "submitted": len(reqs), "bit_exact": ok,
+                        "throughput_rps": len(reqs) / (t_end - t0), "span_s": t_end - t0,
+                        "latency": {"all": pct(allv), "encrypt": pct(lat[0]), "keygen": pct(lat[1]),
+                                    "decrypt": pct(lat[2])},
+                        "ticks": st["ticks"] - t_stat0["ticks"],
+                        "requests_per_tick": len(reqs) / max(1, st["ticks"] - t_stat0["ticks"])})
+    # plain per-call form: one request per tick, run to completion, same kernels
+    sample = make_requests(args.plain_requests, 1000.0)
+    plat = []
+    for req in sample:
+        t_a = S.now()
+        rid = submit(req, t_a)
+        S.drain()
+        good, ms = check(req, rid)
+        plat.append(ms)
+        if req[1] != 2:
+            S.release(rid)
+    plain = {"throughput_rps": 1000.0 * len(plat) / sum(plat), "p50_ms": float(np.percentile(plat, 50)),
+             "p99_ms": float(np.percentile(plat, 99)), "requests": len(plat),
+             "form": "one request per tick, submitted and run to completion before the next"}
+    line = {"workload": "serving", "metric": "requests/s and p50/p99 latency, encrypt:keygen:decrypt = 4:1:4",
+            "unit": "req/s", "n_gpus": 1, "data": "synthetic", "dtype": "uint32",
+            "config": {"tenants": T, "mean_l": float(np.mean(ls)), "n4096_share": float(np.mean(np.array(ns) == 4096)),
+                       "duration_s": args.duration, "arena_gb": args.arena_gb, "tick_gb": args.tick_gb},
+            "results": results, "plain": plain,
+            "bit_exact": all(r["bit_exact"] for r in results)}
+    print(json.dumps(line), flush=True)
+    S.close()
+    return 0 if line["bit_exact"] else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -712,7 +845,13 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="pipeline",
-                    choices=["pipeline", "ntt-sweep", "sampler-sweep", "batched-mixed"])
+                    choices=["pipeline", "ntt-sweep", "sampler-sweep", "batched-mixed", "serving"])
+    ap.add_argument("--tenants", type=int, default=64)
+    ap.add_argument("--rates", type=lambda v: [float(t) for t in v.split(",")], default=[5000, 10000, 20000, 50000])
+    ap.add_argument("--duration", type=float, default=1.0)
+    ap.add_argument("--arena-gb", type=int, default=48)
+    ap.add_argument("--tick-gb", type=int, default=24)
+    ap.add_argument("--plain-requests", type=int, default=100)
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--chunk-gb", type=int, default=24)
     ap.add_argument("--sweep-polys", type=int, default=65536)
@@ -728,6 +867,8 @@ def main():
         return sampler_sweep(args)
     if args.workload == "batched-mixed":
         return batched_mixed(args)
+    if args.workload == "serving":
+        return serving(args)
     return gpu_arm(args)
 
 
