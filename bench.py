@@ -833,6 +833,132 @@ def serving(args):
     return 0 if line["bit_exact"] else 1
 
 
+def _svm_ref_init(path):
+    global _SREF, _SDATA
+    from oracle.ffi import Reference
+    _SREF = Reference("n2048_l124")
+    d = np.load(path)
+    _SDATA = {k: d[k] for k in d.files}
+
+
+def _svm_ref_one(t):
+    """svm_predict3 for one test vector on the reference CPU build: encrypt, then for every
+    support vector keygen + decrypt + GMP decode (y split into y+ - y-, as the reference
+    reduces y as uint32), then the vote"""
+    d = _SDATA
+    ct = _SREF.encrypt(d["x"][t], d["mpk"], d["s2"][t])
+    p = 64 * 124 + 1
+    kv = []
+    for i in range(d["svp"].shape[0]):
+        _, dp = _SREF.decrypt(ct, d["svp"][i], _SREF.keygen(d["svp"][i], d["msk"]))
+        _, dm = _SREF.decrypt(ct, d["svm"][i], _SREF.keygen(d["svm"][i], d["msk"]))
+        v = (int(dp[0]) - int(dm[0])) % p
+        kv.append(v - p if v > p // 2 else v)
+    s = float(np.dot(d["coef"][0][:250], kv[:250]) + np.dot(d["coef"][0][250:], kv[250:])) - float(d["rho"][0])
+    return 1 if s > 0 else -1
+
+
+def svm_workload(args):
+    """Plain IPFE-SVM prediction (the svm_predict3 / svm_predict5 shape): N = 2048, the params.h
+    primes, l = 124 (123 features at 1-based indices), 1,000 test vectors x in {0,1}^123 with 14
+    ones at uniform positions, a linear two-class model of 500 support vectors with integer
+    weights in [-16, 16] (250 per class, sv_coef uniform, rho uniform), data from
+    SplitMix64(0xC0FE0001).  Keys: one master key; the support vectors' function keys are
+    derived once (timed separately).  A step encrypts all 1,000 test vectors and predicts them
+    (coefficient-0 decryption of every (test vector, support vector) pair + the vote).  Every
+    inner product and label of the timed steps is checked against the plaintext model."""
+    import torch
+    import cufe_b200 as cf
+    n, l, ntest, nsv = 2048, 124, 1000, 500
+    rng = np.random.default_rng(splitmix64(0xC0FE0001))
+    x = np.zeros((ntest, l), np.uint32)
+    for t in range(ntest):
+        x[t, 1 + rng.choice(123, 14, replace=False)] = 1
+    sv = np.zeros((nsv, l), np.int32)
+    sv[:, 1:] = rng.integers(-16, 17, (nsv, 123))
+    coef = np.concatenate([rng.uniform(0, 1, 250), -rng.uniform(0, 1, 250)])[None, :]
+    rho = rng.uniform(-1, 1, 1)
+    label = np.array([1, -1], np.int32)
+    seeds_setup = rng.integers(0, 256, (2, 32), dtype=np.uint8)
+    s2 = rng.integers(0, 256, (args.warmup + args.steps, ntest, 32), dtype=np.uint8)
+    torch.cuda.set_device(0)
+    c = cf.Context(n, l)
+    mpk, msk = c.setup(seeds_setup[0], None, seeds_setup[1])
+    t0 = time.perf_counter()
+    m = cf.SvmModel(c, sv, [250, 250], coef, rho, label, msk, signed=True)
+    keys_s = time.perf_counter() - t0
+    xd = cf.to_dev(x)
+    ct = c.ct_buf(ntest)
+    kv = torch.empty((ntest, nsv), dtype=torch.int32, device="cuda:0")
+    labels = torch.empty((args.steps, ntest), dtype=torch.int32, device="cuda:0")
+    kvs = []
+    stream = torch.cuda.current_stream()
+
+    def step(k, out, kvo):
+        c.encrypt(xd, mpk, s2[k], None, ct=ct)
+        m.predict(ct, labels=out, kvalue=kvo)
+
+    for k in range(args.warmup):
+        step(k, labels[0], kv)
+    c.sync()
+    clk = Clocks(0, os.path.join(tempfile.gettempdir(), "cufe_clocks_svm.csv"))
+    c.profile_reset()
+    c.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(args.warmup + k, labels[k], kv)
+        if k == args.steps - 1:
+            kvs.append(kv.clone())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    c.profile(False)
+    prof = c.profile_read()
+    ms = e0.elapsed_time(e1)
+    p = 64 * l + 1
+    ip = x.astype(np.int64) @ sv.astype(np.int64).T
+    kvh = cf.u32(kvs[0]).astype(np.int64)
+    kvh = np.where(kvh > p // 2, kvh - p, kvh)
+    dv = (ip[:, :250].astype(np.float64) @ coef[0][:250] + ip[:, 250:].astype(np.float64) @ coef[0][250:]) - rho[0]
+    want = np.where(dv > 0, 1, -1)
+    ok = bool((kvh == ip).all()) and bool((labels.cpu().numpy() == want[None, :]).all())
+    preds = args.steps * ntest / (ms / 1000.0)
+    line = {"workload": "svm", "metric": "encrypted SVM predictions/s (N=2048, l=124, 500 SVs; bit-exact)",
+            "value": preds, "unit": "predictions/s", "ip_per_s": preds * nsv, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "uint32",
+            "data": "synthetic", "bit_exact": ok, "sv_keys_s": keys_s,
+            "config": {"workload": "1,000 test vectors (a1a-shaped) x 500 support vectors, encrypt + predict per step",
+                       "n": n, "l": l, "test_vectors": ntest, "support_vectors": nsv},
+            "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        import multiprocessing as mp
+        from oracle.ffi import Reference
+        R = Reference("n2048_l124")
+        rmpk, rmsk = R.setup(seeds_setup[0], seeds_setup[1])
+        tmp = tempfile.NamedTemporaryFile(suffix=".npz", delete=False)
+        np.savez(tmp.name, x=x, mpk=rmpk, msk=rmsk, s2=s2[0], svp=np.where(sv > 0, sv, 0).astype(np.uint32),
+                 svm=np.where(sv < 0, -sv, 0).astype(np.uint32), coef=coef, rho=rho)
+        nproc = max(1, min(os.cpu_count() or 1, args.ref_procs))
+        pool = mp.get_context("spawn").Pool(nproc, initializer=_svm_ref_init, initargs=(tmp.name,))
+        try:
+            t0 = time.perf_counter()
+            res = pool.map(_svm_ref_one, list(range(nproc)))
+            dt = time.perf_counter() - t0
+        finally:
+            pool.terminate()
+            os.unlink(tmp.name)
+        line["cpu_baseline"] = {"value": nproc / dt, "unit": "predictions/s", "cores": nproc, "kind": "reference",
+                                "sample": "%d test vectors, one per process: encrypt + 500 x (2 keygens + 2 decrypts "
+                                          "+ GMP decode) + vote (svm_predict3 structure)" % nproc,
+                                "labels_match": bool((np.array(res) == want[:nproc]).all())}
+    print(json.dumps(line), flush=True)
+    m.close()
+    c.close()
+    return 0 if ok else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -845,7 +971,7 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="pipeline",
-                    choices=["pipeline", "ntt-sweep", "sampler-sweep", "batched-mixed", "serving"])
+                    choices=["pipeline", "ntt-sweep", "sampler-sweep", "batched-mixed", "serving", "svm"])
     ap.add_argument("--tenants", type=int, default=64)
     ap.add_argument("--rates", type=lambda v: [float(t) for t in v.split(",")], default=[5000, 10000, 20000, 50000])
     ap.add_argument("--duration", type=float, default=1.0)
@@ -869,6 +995,8 @@ def main():
         return batched_mixed(args)
     if args.workload == "serving":
         return serving(args)
+    if args.workload == "svm":
+        return svm_workload(args)
     return gpu_arm(args)
 
 

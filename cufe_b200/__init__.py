@@ -81,6 +81,9 @@ def lib():
             "cufe_batch_status": [vp],
             "cufe_batch_info": [vp, vp, vp, vp, vp],
             "cufe_batch_instance": [vp, i, vp, vp, vp, vp],
+            "cufe_svm_create": [C.POINTER(vp), vp, i, i, vp, i, vp, vp, vp, vp, vp, vp],
+            "cufe_svm_predict": [vp, i, vp, vp, vp, vp, vp],
+            "cufe_svm_destroy": [vp],
             "cufe_server_create": [C.POINTER(vp), i, vp, vp, C.c_size_t, C.c_size_t, i],
             "cufe_server_destroy": [vp],
             "cufe_server_setup": [vp, vp, vp, vp],
@@ -557,3 +560,45 @@ class Server:
         t, d, f = C.c_longlong(0), C.c_longlong(0), C.c_size_t(0)
         _check(lib().cufe_server_stats(self.h, C.byref(t), C.byref(d), C.byref(f)), "cufe_server_stats")
         return {"ticks": t.value, "done": d.value, "ct_free_bytes": f.value}
+
+
+class SvmModel:
+    """An encrypted linear-SVM predictor on a Context: the support vectors' function keys are
+    derived once; predict() decrypts every (ciphertext, support vector) inner product and takes
+    the libsvm one-against-one vote on the device."""
+
+    def __init__(self, ctx, sv, nsv, sv_coef, rho, label, msk, signed=True, stream=None):
+        self.ctx = ctx
+        sv = np.ascontiguousarray(sv, np.int32)
+        assert sv.ndim == 2 and sv.shape[1] == ctx.l
+        self.lsv = sv.shape[0]
+        self.nr_class = len(nsv)
+        self.npairs = self.nr_class * (self.nr_class - 1) // 2
+        nsv = np.ascontiguousarray(nsv, np.int32)
+        coef = np.ascontiguousarray(sv_coef, np.float64).reshape(self.nr_class - 1, self.lsv)
+        rho = np.ascontiguousarray(rho, np.float64).reshape(self.npairs)
+        label = np.ascontiguousarray(label, np.int32)
+        h = C.c_void_p()
+        _check(lib().cufe_svm_create(C.byref(h), ctx.h, self.nr_class, self.lsv, sv.ctypes.data, int(signed),
+                                     nsv.ctypes.data, coef.ctypes.data, rho.ctypes.data, label.ctypes.data, _ptr(msk),
+                                     _stream(stream, ctx.device)), "cufe_svm_create")
+        self.h = h
+
+    def predict(self, ct, labels=None, kvalue=None, dec=None, stream=None):
+        import torch
+        nct = ct.shape[0]
+        labels = torch.empty(nct, dtype=torch.int32, device=ct.device) if labels is None else labels
+        _check(lib().cufe_svm_predict(self.h, nct, _ptr(ct), _ptr(labels), _ptr(kvalue), _ptr(dec),
+                                      _stream(stream, self.ctx.device)), "cufe_svm_predict")
+        return labels
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cufe_svm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -301,6 +301,56 @@ int cufe_ring_get_variant(const cufe_ring *h, int *fwd, int *inv) {
   return CUFE_OK;
 }
 
+// ------------------------------------------------------------------ encrypted SVM prediction
+
+struct cufe_svm {
+  cufe_ctx *ctx = nullptr;
+  cufe::SvmModel *m = nullptr;
+};
+
+int cufe_svm_create(cufe_svm **out, cufe_ctx *h, int nr_class, int nsv_total, const int32_t *sv, int sv_signed,
+                    const int *nsv, const double *sv_coef, const double *rho, const int *label, const uint32_t *d_msk,
+                    void *stream) {
+  if (!out || !h) return CUFE_ERR_INVALID;
+  *out = nullptr;
+  cufe_svm *sm = new cufe_svm;
+  sm->ctx = h;
+  sm->m = cufe::svm_new();
+  int rc;
+  {
+    std::lock_guard<std::mutex> lk(h->c.mu);
+    ProfBind pb(&h->c.prof);
+    if (cudaSetDevice(h->c.device) != cudaSuccess) {
+      rc = CUFE_ERR_CUDA;
+    } else {
+      rc = cufe::svm_create(h->c, *sm->m, nr_class, nsv_total, sv, sv_signed, nsv, sv_coef, rho, label, d_msk,
+                            h->c.pick(stream));
+    }
+  }
+  if (rc) {
+    cufe::svm_delete(sm->m);
+    delete sm;
+    return rc;
+  }
+  *out = sm;
+  return CUFE_OK;
+}
+
+int cufe_svm_predict(cufe_svm *sm, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kvalue, double *d_dec,
+                     void *stream) {
+  if (!sm) return CUFE_ERR_INVALID;
+  cufe_ctx *h = sm->ctx;
+  CTX_CALL(h, cufe::svm_predict(h->c, *sm->m, nct, d_ct, d_label, d_kvalue, d_dec, h->c.pick(stream)));
+}
+
+int cufe_svm_destroy(cufe_svm *sm) {
+  if (!sm) return CUFE_ERR_INVALID;
+  cudaSetDevice(sm->ctx->c.device);
+  cufe::svm_delete(sm->m);
+  delete sm;
+  return CUFE_OK;
+}
+
 // ------------------------------------------------------------------ reference drop-in
 
 namespace {

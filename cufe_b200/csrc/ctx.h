@@ -76,6 +76,13 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
 int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                         const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s);
 int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s);
+struct SvmModel;
+int svm_create(Ctx &c, SvmModel &m, int nr_class, int lsv, const int32_t *sv, int y_signed, const int *nsv,
+               const double *sv_coef, const double *rho, const int *label, const uint32_t *d_msk, cudaStream_t s);
+int svm_predict(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kval, double *d_dec,
+                cudaStream_t s);
+SvmModel *svm_new();
+void svm_delete(SvmModel *m);
 int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                       const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s);
 int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,

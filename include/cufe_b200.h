@@ -161,6 +161,31 @@ int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0
 int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void *stream);
 
 /* =====================================================================================
+ * 2a. Encrypted linear-SVM prediction: the svm_predict5 path (svm_predict_gpu,
+ *     main.c:270-390) with the support vectors' function keys derived once and resident.
+ * ===================================================================================== */
+
+typedef struct cufe_svm cufe_svm;
+
+/* A libsvm one-against-one model (svm/svm.h:52-72) on the context's parameters: nr_class
+ * classes, nsv_total support vectors sv[nsv_total][l] (convertToarray's dense layout,
+ * main.c:30-41: feature index -> value, zero elsewhere; sv_signed = 1 allows negative
+ * integer entries, 0 is the reference's uint32), nSV[nr_class], sv_coef[nr_class-1][nsv_total],
+ * rho[nr_class*(nr_class-1)/2], label[nr_class]; d_msk the master secret key.  Derives the
+ * function key of every support vector once (rlwe_sife_keygen, src/rlwe_sife.c:215-245);
+ * synchronous. */
+int cufe_svm_create(cufe_svm **svm, cufe_ctx *ctx, int nr_class, int nsv_total, const int32_t *sv, int sv_signed,
+                    const int *nsv, const double *sv_coef, const double *rho, const int *label, const uint32_t *d_msk,
+                    void *stream);
+/* Predict nct encrypted test vectors d_ct[nct][l+1][3][n]: kvalue = decoded coefficient 0
+ * of every (ciphertext, support vector) decryption, then the vote of main.c:331-379 with
+ * fused multiply-adds in the reference's order.  d_label[nct] (device); d_kvalue
+ * [nct][nsv_total] and d_dec [nct][pairs] are optional (device, NULL to skip). */
+int cufe_svm_predict(cufe_svm *svm, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kvalue, double *d_dec,
+                     void *stream);
+int cufe_svm_destroy(cufe_svm *svm);
+
+/* =====================================================================================
  * 2b. Heterogeneous batches: many independent instances, each with its own ring degree n_i,
  *     vector length l_i (hence its own p_i = 64 l_i + 1 and floor(q / p_i), src/params.h:26-27)
  *     and master key pair.  No counterpart in the reference, which runs one instance of
