@@ -433,11 +433,13 @@ def gpu_arm(args):
             "share": tot / sum(v[1] for v in prof.values())}
     roof["frac"] = roof["achieved"] / hbm_peak if roof["achieved"] else None
     if name.startswith("sample_cand"):
-        # the AES keystream bounds this kernel: 15 AES-256 blocks per refill, each
-        # 14 rounds x 16 T-table lookups from shared memory (one warp LDS per clock per SM)
+        # the AES keystream bounds this kernel: 15 AES-256 blocks per refill; with the
+        # counter caching a block takes 1 + 4 + 11 x 16 + 16 = 197 T-table lookups from
+        # shared memory, plus 15 per refill for the round-2 constants (one warp LDS per clock
+        # per SM): 198 per block
         blocks = refills3 * B * 15
         sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
-        lds_peak = 148 * sm_mhz * 1e6 * 32 / (14 * 16)
+        lds_peak = 148 * sm_mhz * 1e6 * 32 / 198
         roof["pipe"] = {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)",
                         "achieved": blocks / per_launch_s, "peak_lds_bound": lds_peak,
                         "frac": blocks / per_launch_s / lds_peak, "sm_mhz": sm_mhz}

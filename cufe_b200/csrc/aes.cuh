@@ -50,11 +50,12 @@ __device__ __forceinline__ uint32_t taddr(const AesCtx &c, uint32_t s) {
   return __byte_perm(s, c.laneoff, 0x5504 | (B << 4));
 }
 
-// rounds 1..14 on a state that already holds input ^ rk[0..3]
-__device__ __forceinline__ void aes256_rounds(uint32_t &s0, uint32_t &s1, uint32_t &s2, uint32_t &s3,
-                                              const uint32_t (&rk)[60], const AesCtx &c) {
+// rounds R0..14 on the state after round R0 - 1 (R0 = 1: after the initial AddRoundKey)
+template <int R0>
+__device__ __forceinline__ void aes256_rounds_from(uint32_t &s0, uint32_t &s1, uint32_t &s2, uint32_t &s3,
+                                                   const uint32_t (&rk)[60], const AesCtx &c) {
 #pragma unroll
-  for (int r = 1; r < 14; ++r) {
+  for (int r = R0; r < 14; ++r) {
     const uint32_t t0 = te<0>(c, taddr<3>(c, s0)) ^ te<1>(c, taddr<2>(c, s1)) ^
                         te<2>(c, taddr<1>(c, s2)) ^ te<3>(c, taddr<0>(c, s3)) ^ rk[4 * r];
     const uint32_t t1 = te<0>(c, taddr<3>(c, s1)) ^ te<1>(c, taddr<2>(c, s2)) ^
@@ -81,6 +82,57 @@ __device__ __forceinline__ void aes256_rounds(uint32_t &s0, uint32_t &s1, uint32
   s1 = o1;
   s2 = o2;
   s3 = o3;
+}
+
+// rounds 1..14 on a state that already holds input ^ rk[0..3]
+__device__ __forceinline__ void aes256_rounds(uint32_t &s0, uint32_t &s1, uint32_t &s2, uint32_t &s3,
+                                              const uint32_t (&rk)[60], const AesCtx &c) {
+  aes256_rounds_from<1>(s0, s1, s2, s3, rk, c);
+}
+
+// Counter caching for the CPU mapping with nonce 0: the input block is 0^12 || BE32(ctr), so
+// after the initial AddRoundKey only state word 3 depends on ctr.  In round 1 each output
+// word takes exactly one byte of word 3 (T3 of its low byte for word 0, T2/T1/T0 of the
+// higher bytes for words 1..3); for counters with equal upper 24 bits, words 1..3 after round
+// 1 are therefore fixed and only word 0 varies, and in round 2 each output word takes one byte
+// of word 0 and three fixed bytes.  k0..k3: the ctr-independent part of round 1 (per key);
+// c0..c3: the fixed part of round 2 for the upper counter bits `hi` (recomputed when they
+// change).  Per block, rounds 1 and 2 then take 1 + 4 table lookups instead of 32.
+struct CtrCache {
+  uint32_t k0, k1, k2, k3, c0, c1, c2, c3, hi;
+};
+
+__device__ __forceinline__ void ctr_cache_key(CtrCache &cc, const uint32_t (&rk)[60], const AesCtx &c) {
+  const uint32_t s0 = rk[0], s1 = rk[1], s2 = rk[2];
+  cc.k0 = te<0>(c, taddr<3>(c, s0)) ^ te<1>(c, taddr<2>(c, s1)) ^ te<2>(c, taddr<1>(c, s2)) ^ rk[4];
+  cc.k1 = te<0>(c, taddr<3>(c, s1)) ^ te<1>(c, taddr<2>(c, s2)) ^ te<3>(c, taddr<0>(c, s0)) ^ rk[5];
+  cc.k2 = te<0>(c, taddr<3>(c, s2)) ^ te<2>(c, taddr<1>(c, s0)) ^ te<3>(c, taddr<0>(c, s1)) ^ rk[6];
+  cc.k3 = te<1>(c, taddr<2>(c, s0)) ^ te<2>(c, taddr<1>(c, s1)) ^ te<3>(c, taddr<0>(c, s2)) ^ rk[7];
+  cc.hi = 0xffffffffu;  // no counter cached
+}
+
+// the keystream block of counter ctr (nonce 0), output as in aes256_ctr_block
+__device__ __forceinline__ void aes256_ctr_block_cached(uint32_t (&o)[4], uint32_t ctr, const uint32_t (&rk)[60],
+                                                        const AesCtx &c, CtrCache &cc) {
+  const uint32_t w3 = ctr ^ rk[3];
+  if ((ctr >> 8) != cc.hi) {
+    cc.hi = ctr >> 8;
+    const uint32_t u1 = cc.k1 ^ te<2>(c, taddr<1>(c, w3));
+    const uint32_t u2 = cc.k2 ^ te<1>(c, taddr<2>(c, w3));
+    const uint32_t u3 = cc.k3 ^ te<0>(c, taddr<3>(c, w3));
+    cc.c0 = te<1>(c, taddr<2>(c, u1)) ^ te<2>(c, taddr<1>(c, u2)) ^ te<3>(c, taddr<0>(c, u3)) ^ rk[8];
+    cc.c1 = te<0>(c, taddr<3>(c, u1)) ^ te<1>(c, taddr<2>(c, u2)) ^ te<2>(c, taddr<1>(c, u3)) ^ rk[9];
+    cc.c2 = te<0>(c, taddr<3>(c, u2)) ^ te<1>(c, taddr<2>(c, u3)) ^ te<3>(c, taddr<0>(c, u1)) ^ rk[10];
+    cc.c3 = te<0>(c, taddr<3>(c, u3)) ^ te<2>(c, taddr<1>(c, u1)) ^ te<3>(c, taddr<0>(c, u2)) ^ rk[11];
+  }
+  const uint32_t a0 = cc.k0 ^ te<3>(c, taddr<0>(c, w3));
+  uint32_t s0 = cc.c0 ^ te<0>(c, taddr<3>(c, a0)), s1 = cc.c1 ^ te<3>(c, taddr<0>(c, a0));
+  uint32_t s2 = cc.c2 ^ te<2>(c, taddr<1>(c, a0)), s3 = cc.c3 ^ te<1>(c, taddr<2>(c, a0));
+  aes256_rounds_from<3>(s0, s1, s2, s3, rk, c);
+  o[0] = s0;
+  o[1] = s1;
+  o[2] = s2;
+  o[3] = s3;
 }
 
 // One keystream block of the CPU counter mapping (src/aes256ctr.c:13-81): input

@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(kCandThreads, 1)
   uint32_t rk[60];
   uint32_t st = 0;
   uint32_t lo = 1, hi = 0;  // refill range of stream st (empty: forces the first lookup)
+  CtrCache cc;
   const uint32_t *rkg = rkeys;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     if (g < lo || g >= hi) {
@@ -127,6 +128,7 @@ __global__ void __launch_bounds__(kCandThreads, 1)
       rkg = rkeys + (size_t)st * 60;
 #pragma unroll
       for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
+      ctr_cache_key(cc, rk, c);
     }
     const uint32_t t = g - lo;
     const uint32_t cb = t * 24u;
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(kCandThreads, 1)
 #pragma unroll 1
     for (int bi = 0; bi < kRefillBlocks; ++bi) {
       uint32_t W[4];
-      aes256_ctr_block(W, 0u, cb + c_refill_blocks[bi], rk, c);
+      aes256_ctr_block_cached(W, cb + c_refill_blocks[bi], rk, c, cc);
       buf4[bi] = make_uint4(W[0], W[1], W[2], W[3]);
     }
     const uint32_t *buf = reinterpret_cast<const uint32_t *>(buf4);
