@@ -433,11 +433,11 @@ def gpu_arm(args):
             "share": tot / sum(v[1] for v in prof.values())}
     roof["frac"] = roof["achieved"] / hbm_peak if roof["achieved"] else None
     if name.startswith("sample_cand"):
-        # the AES keystream bounds this kernel: 15 AES-256 blocks per refill; with the
+        # the AES keystream bounds this kernel: 14 AES-256 blocks per refill; with the
         # counter caching a block takes 1 + 4 + 11 x 16 + 16 = 197 T-table lookups from
         # shared memory, plus 15 per refill for the round-2 constants (one warp LDS per clock
         # per SM): 198 per block
-        blocks = refills3 * B * 15
+        blocks = refills3 * B * 14
         sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
         lds_peak = 148 * sm_mhz * 1e6 * 32 / 198
         roof["pipe"] = {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)",
@@ -502,8 +502,8 @@ def ntt_sweep(args):
     stream = torch.cuda.current_stream()
     clk = Clocks(0, os.path.join(tempfile.gettempdir(), "cufe_clocks_sweep.csv"))
     rows = []
-    for n in (1024, 2048, 4096, 8192):
-        for k in (3, 4, 5, 6):
+    for n in args.sweep_n:
+        for k in args.sweep_k:
             ring = cf.Ring(n, k)
             data = torch.empty((npoly, k, n), dtype=torch.int32, device=dev)
             for j in range(k):
@@ -513,7 +513,7 @@ def ntt_sweep(args):
             nbytes = 8 * n * npoly * k
             per_variant = {}
             ok = True
-            for var in (1, 2, 3):
+            for var in args.sweep_variants:
                 ring.set_variant(var, var)
                 for _ in range(args.warmup):
                     ring.forward(data)
@@ -533,6 +533,9 @@ def ntt_sweep(args):
                 per_variant[var] = (float(np.median(fwd)), float(np.median(inv)))
             tuned = ring.tune(npoly)
             fv, iv = tuned["variant"]
+            if fv not in per_variant or iv not in per_variant:  # a variant left out of the sweep
+                fv, iv = (min(per_variant, key=lambda v: per_variant[v][0]),
+                          min(per_variant, key=lambda v: per_variant[v][1]))
             f_ms, i_ms = per_variant[fv][0], per_variant[iv][1]
             rows.append({"n": n, "k": k, "bytes_per_pass": nbytes, "fwd_ms": f_ms, "inv_ms": i_ms,
                          "fwd_gbs": nbytes / f_ms / 1e6, "inv_gbs": nbytes / i_ms / 1e6,
@@ -984,6 +987,10 @@ def main():
     ap.add_argument("--chunk-gb", type=int, default=24)
     ap.add_argument("--sweep-polys", type=int, default=65536)
     ap.add_argument("--sweep-samples", type=int, default=2 ** 30)
+    ints = lambda v: [int(t) for t in v.split(",")]  # noqa: E731
+    ap.add_argument("--sweep-n", type=ints, default=[1024, 2048, 4096, 8192])
+    ap.add_argument("--sweep-k", type=ints, default=[3, 4, 5, 6])
+    ap.add_argument("--sweep-variants", type=ints, default=[1, 2, 3])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

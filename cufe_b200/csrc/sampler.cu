@@ -92,15 +92,19 @@ __device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb,
   return cdt_sample<false>(r2, 0);
 }
 
-// Blocks of one refill that the reference reads (16-byte block b = bytes 16b..16b+15):
-// 2, 3 (CDT high words of lanes 0..3, bytes 32..63), 4, 5, 6 (Bernoulli bytes 64..99),
-// 8..12 (CDT high words and Bernoulli bytes of lanes 4..7, 132..199), 12..17 (uniform words
-// from byte 200, sign byte 280).  Blocks 0, 1, 7 hold only the low CDT words, which S1/S2
-// never use and S3 uses only on ties (regenerated then).  kBufBlock lists them in buffer
-// order; word w of the refill (bytes 4w..4w+3) is buffer word kbuf(w).
-constexpr int kRefillBlocks = 15;
-__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17};
-__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : w - 12; }
+// Blocks of one refill that the fast path reads (16-byte block b = bytes 16b..16b+15, word w
+// = bytes 4w..4w+3): 2, 3 (CDT high words of lanes 0..3, words 8..15), 4, 5, 6 (Bernoulli
+// words 16..24), 8..12 (CDT high words and Bernoulli words of lanes 4..7, words 33..49),
+// 12..15 (the first 12 uniform words from byte 200, words 50..61) and 17 (sign byte 280,
+// word 70).  Blocks 0, 1, 7 hold only the low CDT words, which S1/S2 never use and S3 uses
+// only on ties; block 16 holds uniform words 64..67, needed only when fewer than 8 of the
+// first 12 words are accepted.  Both rare cases regenerate what they need on their slow
+// paths.  Buffer word kbuf(w) holds refill word w.
+constexpr int kRefillBlocks = 14;
+__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 15, 17};
+__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : (w < 64 ? w - 12 : w - 16); }
+static_assert(kbuf(70) == 4 * 13 + 2, "sign word lives in block 17, the last buffer block");
+static_assert(kbuf(61) == 4 * 12 + 1, "uniform words end in block 15");
 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
 constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed with p < 1e-7
