@@ -207,10 +207,10 @@ def cpu_baseline_sample(x, y, seeds2, setup_seeds, nproc, steps=2):
 # ----------------------------------------------------------------------------- GPU arm
 
 # DRAM bytes per refill of the sigma_3 candidate kernel, from one ncu capture of a batch-16
-# launch (dram__bytes_read.sum + dram__bytes_write.sum = 3.71 MB + 1402.23 MB over
+# launch (dram__bytes_read.sum + dram__bytes_write.sum = 0.26 MB + 1301.44 MB over
 # 16 x 1,103,616 refills); traffic grows with the refill count, so a launch of B streams
 # moves B x refills x this
-CAND_S3_DRAM_BYTES_PER_REFILL = (3.708416e6 + 1402.233648e6) / (16 * 1103616)
+CAND_S3_DRAM_BYTES_PER_REFILL = (0.257792e6 + 1301.437e6) / (16 * 1103616)
 
 
 # algorithmic HBM bytes per launch of each kernel at this workload (batch B)
