@@ -28,34 +28,48 @@ struct NttPlan {
   static constexpr int SMEM_WORDS = N;
   __host__ __device__ static constexpr int radix_bits(int p) { return p == 0 ? R0 : 4; }
   __host__ __device__ static constexpr int first_stage(int p) { return p == 0 ? 0 : R0 + 4 * (p - 1); }
-  // coefficient index held in register e by thread th during pass PASS
+  // coefficient index held in register e by thread th during pass PASS.  The bits that come
+  // from th and the bits that come from e are disjoint, so idx = idx_th(th) + idx_e(e), the
+  // second a compile-time constant (an immediate offset in every load and store).
   template <int PASS>
-  __device__ __forceinline__ static int idx(int th, int e) {
+  __device__ __forceinline__ static int idx_th(int th) {
     constexpr int rb = radix_bits(PASS), s0 = first_stage(PASS);
     constexpr int plo = LOGN - s0 - rb, phi = LOGN - 1 - s0;
-    const int v = e >> rb, M = e & ((1 << rb) - 1);
-    const int U = v * T + th;
-    const int H = U >> plo, L = U & ((1 << plo) - 1);
-    return (H << (phi + 1)) | (M << plo) | L;
+    return ((th >> plo) << (phi + 1)) | (th & ((1 << plo) - 1));
   }
-  __device__ __forceinline__ static int swz(int j) { return j ^ ((j >> 4) & 31); }
+  template <int PASS>
+  __host__ __device__ static constexpr int idx_e(int e) {
+    constexpr int rb = radix_bits(PASS), s0 = first_stage(PASS);
+    constexpr int plo = LOGN - s0 - rb, phi = LOGN - 1 - s0;
+    return ((((e >> rb) * T) >> plo) << (phi + 1)) | ((e & ((1 << rb) - 1)) << plo) | (((e >> rb) * T) & ((1 << plo) - 1));
+  }
+  template <int PASS>
+  __device__ __forceinline__ static int idx(int th, int e) {
+    return idx_th<PASS>(th) + idx_e<PASS>(e);
+  }
+  __host__ __device__ static constexpr int swz(int j) { return j ^ ((j >> 4) & 31); }
 };
 
 // P residue polynomials per thread group (same modulus, shared twiddles and addresses):
 // polynomial p uses registers a[p][] and shared words sm[p * N ...]
+// The swizzle is linear over XOR and idx_th / idx_e have disjoint bits, so the swizzled
+// address of register e is swz(idx_th(th)) ^ swz(idx_e(e)): one per-thread base and one XOR
+// with a constant per access.
 template <int LOGN, int FROM, int TO, int P_>
 __device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][16], uint32_t *sm, int th) {
   using P = NttPlan<LOGN>;
+  const int wb = P::swz(P::template idx_th<FROM>(th));
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    const int j = P::swz(P::template idx<FROM>(th, e));
+    const int j = wb ^ P::swz(P::template idx_e<FROM>(e));
 #pragma unroll
     for (int p = 0; p < P_; ++p) sm[p * P::N + j] = a[p][e];
   }
   __syncthreads();
+  const int rbase = P::swz(P::template idx_th<TO>(th));
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    const int j = P::swz(P::template idx<TO>(th, e));
+    const int j = rbase ^ P::swz(P::template idx_e<TO>(e));
 #pragma unroll
     for (int p = 0; p < P_; ++p) a[p][e] = sm[p * P::N + j];
   }
