@@ -99,6 +99,7 @@ def lib():
             "cufe_ring_set_variant": [vp, i, i],
             "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
+            "cufe_sampler_call_search": [i],
             "cufe_dropin_configure": [i, i, i],
             "cufe_dropin_status": [],
             "rlwe_sife_setup_gpu": [vp, vp, vp, vp, vp],

@@ -964,6 +964,9 @@ struct Server {
       uint32_t *rhsh = reinterpret_cast<uint32_t *>(take(w_rh * 4));
       uint32_t *f3 = reinterpret_cast<uint32_t *>(take(w_f3 * 4));
       uint32_t *rk = reinterpret_cast<uint32_t *>(take((size_t)2 * ne * 60 * 4));
+      const size_t before = (size_t)(p - d_scr);
+      if (before + std::max(seg_scratch_bytes(z2), seg_scratch_bytes(z3)) > scr_bytes)
+        z2.doubling = z3.doubling = false;  // no room for the doubling tables: serial walk
       void *samp = take(std::max(seg_scratch_bytes(z2), seg_scratch_bytes(z3)));
       if ((size_t)(p - d_scr) > scr_bytes) {
         set_last_error("server: tick scratch exceeded");

@@ -301,6 +301,12 @@ int cufe_ring_get_variant(const cufe_ring *h, int *fwd, int *inv) {
   return CUFE_OK;
 }
 
+int cufe_sampler_call_search(int mode) {
+  if (mode < 0 || mode > 1) return CUFE_ERR_INVALID;
+  cufe::set_call_search(mode);
+  return CUFE_OK;
+}
+
 // ------------------------------------------------------------------ encrypted SVM prediction
 
 struct cufe_svm {

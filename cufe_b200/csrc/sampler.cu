@@ -360,6 +360,67 @@ __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__re
   }
 }
 
+// Pointer doubling for the call starts (the same result as k_walk).  next(t) of stream s is
+// the refill after a call that starts at refill t ends: e + 1 for the first e >= t whose
+// inclusive prefix reaches E(t) + n, or R + 1 (absorbing) when the stream runs out; the start
+// of call c is next applied c times to 0, assembled from the bits of c with the tables
+// J_k = next^(2^k).
+__global__ void k_next_start(const uint32_t *__restrict__ elocal, const uint32_t *__restrict__ tile_off,
+                             const uint8_t *__restrict__ amask, SegDev sg, float mean_accept,
+                             uint32_t *__restrict__ next) {
+  const uint64_t total = __ldg(sg.roff + sg.nstreams);
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const uint32_t st = seg_find(sg.roff, sg.nstreams, g);
+  const SegView v = seg_view(sg, st);
+  const uint32_t t = (uint32_t)(g - v.r0), n = __ldg(sg.n + st);
+  const uint32_t target = prefix_at(elocal, tile_off, amask, v, t) + n;
+  // smallest e in [t, R) with E(e + 1) >= target; try the expected call length first
+  uint32_t lo = t, hi = v.R;
+  const uint32_t guess = t + 2u * (uint32_t)((float)n / mean_accept) + 64u;
+  if (guess < v.R && prefix_at(elocal, tile_off, amask, v, guess + 1) >= target) hi = guess;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (prefix_at(elocal, tile_off, amask, v, mid + 1) >= target) hi = mid;
+    else lo = mid + 1;
+  }
+  next[g] = lo < v.R ? lo + 1 : v.R + 1;
+}
+
+__global__ void k_next_square(const uint32_t *__restrict__ jin, uint32_t *__restrict__ jout, SegDev sg) {
+  const uint64_t total = __ldg(sg.roff + sg.nstreams);
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const uint32_t st = seg_find(sg.roff, sg.nstreams, g);
+  const uint64_t r0 = __ldg(sg.roff + st);
+  const uint32_t R = (uint32_t)(__ldg(sg.roff + st + 1) - r0);
+  const uint32_t a = jin[g];
+  jout[g] = a < R ? jin[r0 + a] : R + 1;
+}
+
+// one thread per (stream, c), c = 0 .. calls: call_start[coff[s] + s + c]
+__global__ void k_starts_from_tables(const uint32_t *__restrict__ tables, int levels, uint64_t refills, SegDev sg,
+                                     uint32_t *__restrict__ call_start, uint32_t *__restrict__ status) {
+  const uint64_t total = __ldg(sg.coff + sg.nstreams) + sg.nstreams;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  uint32_t lo = 0, hi = sg.nstreams;  // stream s owns entries [coff[s] + s, coff[s+1] + s + 1)
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(sg.coff + mid) + mid <= i) lo = mid;
+    else hi = mid;
+  }
+  const uint32_t st = lo;
+  const uint32_t c = (uint32_t)(i - (__ldg(sg.coff + st) + st));
+  const uint64_t r0 = __ldg(sg.roff + st);
+  const uint32_t R = (uint32_t)(__ldg(sg.roff + st + 1) - r0);
+  uint32_t a = 0;
+  for (int k = 0; k < levels; ++k)
+    if ((c >> k) & 1u) a = a < R ? tables[(uint64_t)k * refills + r0 + a] : R + 1;
+  call_start[i] = a <= R ? a : R;
+  if (a > R && c == __ldg(sg.calls + st)) atomicOr(status, kStatusRefillsExhausted);
+}
+
 // ------------------------------------------------------------------ CPU mapping, phase 3
 
 struct ModArgs {
@@ -734,7 +795,7 @@ SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_
   uint32_t *ht = reinterpret_cast<uint32_t *>(b + L.toff);
   uint64_t *hr = reinterpret_cast<uint64_t *>(b + L.roff), *hco = reinterpret_cast<uint64_t *>(b + L.coff);
   uint64_t *ho = reinterpret_cast<uint64_t *>(b + L.ooff);
-  SegSizes z{S, 0, 0, 0};
+  SegSizes z{S, 0, 0, 0, 0, false};
   for (uint32_t i = 0; i < S; ++i) {
     const uint32_t R = cpu_map_refills(calls[i], n[i], sig);
     hn[i] = n[i];
@@ -746,21 +807,39 @@ SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_
     z.refills += R;
     z.tiles += (R + kScanTile - 1) / kScanTile;
     z.calls += calls[i];
+    z.max_calls = std::max(z.max_calls, calls[i]);
   }
   hr[S] = z.refills;
   ht[S] = z.tiles;
   hco[S] = z.calls;
+  z.doubling = seg_auto_doubling(z.refills);
   return z;
 }
 
 static SegSizes seg_uniform_sizes(uint32_t S, uint32_t calls, uint32_t n, int sig) {
   const uint32_t R = cpu_map_refills(calls, n, sig);
-  return SegSizes{S, (uint64_t)S * R, S * ((R + kScanTile - 1) / kScanTile), (uint64_t)S * calls};
+  return SegSizes{S, (uint64_t)S * R, S * ((R + kScanTile - 1) / kScanTile), (uint64_t)S * calls, calls,
+                  seg_auto_doubling((uint64_t)S * R)};
 }
 
+static int g_call_search = 0;
+void set_call_search(int mode) { g_call_search = mode; }
+int get_call_search() { return g_call_search; }
+
+constexpr uint64_t kDoublingMaxRefills = (uint64_t)32 << 20;
+
+static int doubling_levels(uint32_t max_calls) {
+  int k = 1;
+  while (k < 31 && (1u << k) <= max_calls) ++k;
+  return k;  // bit_length(max_calls), at least 1
+}
+bool seg_auto_doubling(uint64_t refills) { return g_call_search != 1 && refills <= kDoublingMaxRefills; }
+
 size_t seg_scratch_bytes(const SegSizes &z) {
-  return align256(z.refills * 64) + align256(z.refills) + align256(z.refills * 4) + align256((size_t)z.tiles * 4) +
-         align256((z.calls + z.nstreams) * 4);
+  size_t b = align256(z.refills * 64) + align256(z.refills) + align256(z.refills * 4) + align256((size_t)z.tiles * 4) +
+             align256((z.calls + z.nstreams) * 4);
+  if (z.doubling) b += (size_t)doubling_levels(z.max_calls) * align256(z.refills * 4);
+  return b;
 }
 
 size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, int sig) {
@@ -801,7 +880,17 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
     k_scan_tiles<<<z.tiles, 512, 0, s>>>(amask, sg, elocal, tsum);
     k_scan_sums<<<z.nstreams, 1024, 0, s>>>(tsum, sg);
   }
-  {
+  if (z.doubling) {
+    const int levels = doubling_levels(z.max_calls);
+    uint32_t *tab = reinterpret_cast<uint32_t *>(take((size_t)levels * align256(z.refills * 4)));
+    const uint64_t stride = align256(z.refills * 4) / 4;
+    ProfScope ps("sample_walk", s);
+    const unsigned rg = (unsigned)((z.refills + 255) / 256);
+    k_next_start<<<rg, 256, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), tab);
+    for (int k = 1; k < levels; ++k) k_next_square<<<rg, 256, 0, s>>>(tab + (k - 1) * stride, tab + k * stride, sg);
+    k_starts_from_tables<<<(unsigned)((z.calls + z.nstreams + 255) / 256), 256, 0, s>>>(tab, levels, stride, sg,
+                                                                                        cstart, d_status);
+  } else {
     ProfScope ps("sample_walk", s);
     k_walk<<<(z.nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), cstart, d_status);
   }

@@ -42,7 +42,16 @@ struct SegSizes {
   uint64_t refills;
   uint32_t tiles;
   uint64_t calls;
+  uint32_t max_calls;  // the largest calls[s]
+  bool doubling;       // call starts by pointer doubling (its tables are part of the scratch)
 };
+// How the call starts of the CPU mapping are found.  Pointer doubling is parallel over
+// refills and calls but needs bit_length(max_calls) words per refill of scratch, so it is
+// chosen up to 32 Mi refills; the serial walk (one warp per stream) otherwise, or always
+// after set_call_search(1).  The choice is fixed in SegSizes when a scratch is sized.
+void set_call_search(int mode);
+int get_call_search();
+bool seg_auto_doubling(uint64_t refills);
 struct SegLayout {
   size_t n, calls, toff, roff, coff, ooff, bytes;
 };

@@ -160,6 +160,12 @@ int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0
 /* sample_polya (src/sample.c:56-128): d_a[3][n] */
 int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void *stream);
 
+/* How the CPU-mapping samplers find where each gaussian_sampler_S* call starts (process-wide;
+ * both give the same samples): 0 (default) pointer doubling for runs up to 32 Mi refills,
+ * the serial walk above; 1 always the serial walk.  Applies to workspaces sized after the
+ * call. */
+int cufe_sampler_call_search(int mode);
+
 /* =====================================================================================
  * 2a. Encrypted linear-SVM prediction: the svm_predict5 path (svm_predict_gpu,
  *     main.c:270-390) with the support vectors' function keys derived once and resident.

@@ -101,6 +101,43 @@ def test_sampler_cpu_map(sig, rng, oracle_built):
 
 
 @pytest.mark.parametrize("sig", [0, 1, 2])
+def test_call_search_walk_equals_doubling(sig, rng, oracle_built):
+    """the two call-start searches give the same samples (uniform streams, and uneven ones
+    through a heterogeneous batch)"""
+    L = cf.lib()
+    c = cf.Context(1024, 8)
+    keys = seeds(rng, 5)
+    outs = []
+    for mode in (0, 1):
+        assert L.cufe_sampler_call_search(mode) == 0
+        outs.append(cf.u32(c.sample_cpu_map(sig, keys, 37)))
+        c.sync()
+    assert L.cufe_sampler_call_search(0) == 0
+    assert (outs[0] == outs[1]).all()
+    c.close()
+    if sig == 2:
+        ns, ls = [256, 1024, 512], [5, 33, 12]
+        res = []
+        for mode in (0, 1):
+            L.cufe_sampler_call_search(mode)
+            B = cf.Batch(ns, ls)
+            r = np.random.default_rng(9)
+            B.setup(r.integers(0, 256, (3, 32), dtype=np.uint8), None, r.integers(0, 256, (3, 32), dtype=np.uint8))
+            x = dev(B.pack([r.integers(0, 5, l) for l in ls]).astype(np.uint32))
+            y = dev(B.pack([r.integers(-16, 17, l) for l in ls]).astype(np.int32))
+            d0 = dev(np.zeros((3, 3), np.uint32))
+            B.bind(x, y, cf.bytes_to_dev(r.integers(0, 256, (3, 32), dtype=np.uint8)),
+                   cf.bytes_to_dev(r.integers(0, 256, (3, 32), dtype=np.uint8)), d0=d0)
+            B.run()
+            torch.cuda.synchronize()
+            res.append([B.fetch(B.instance(i)[3], (l + 1) * 3 * n) for i, (n, l) in enumerate(zip(ns, ls))])
+            B.close()
+        L.cufe_sampler_call_search(0)
+        for a, b in zip(*res):
+            assert (a == b).all()
+
+
+@pytest.mark.parametrize("sig", [0, 1, 2])
 def test_sampler_gpu_map(sig, rng, oracle_built):
     n = 4096
     c = cf.Context(n, 4)
