@@ -82,3 +82,28 @@ def test_svm_predict(nsv, signed, rng, oracle_built):
                 assert int(O.decode(O.decrypt(rct, y, O.keygen(y, rmsk)))[0]) == int(kvh[t, i])
     m.close()
     c.close()
+
+
+def test_svm_from_libsvm_file(tmp_path, rng, oracle_built):
+    """a model file in libsvm's format, loaded and quantized, predicts like the plaintext vote"""
+    from cufe_b200 import libsvm
+    n, l = 1024, 40
+    nsv = [7, 5, 6]
+    sv = rng.uniform(-2, 2, (sum(nsv), l))
+    sv[:, 0] = 0
+    coef = rng.uniform(-1, 1, (2, sum(nsv)))
+    path = str(tmp_path / "m.model")
+    libsvm.save_model(path, 3, sv, nsv, coef, rng.uniform(-0.5, 0.5, 3), [1, 2, 3])
+    svq, nr_sv, c_, rho, label, _ = libsvm.to_integer(libsvm.load_model(path), l)
+    ctx = cf.Context(n, l)
+    mpk, msk = ctx.setup(*seeds(rng, 1), None, seeds(rng, 1)[0])
+    # binary features (a1a-like): |<x, sv>| <= 16 l < p / 2, where the centred decode is exact
+    x = rng.integers(0, 2, (20, l)).astype(np.uint32)
+    x[:, 0] = 0
+    m = cf.SvmModel(ctx, svq, nr_sv, c_, rho, label, msk, signed=True)
+    got = m.predict(ctx.encrypt(cf.to_dev(x), mpk, seeds(rng, 20), None))
+    ctx.sync()
+    want, _ = plain_vote((x.astype(np.int64) @ svq.astype(np.int64).T).astype(np.float64), nr_sv, c_, rho, label)
+    assert (got.cpu().numpy() == want).all()
+    m.close()
+    ctx.close()
