@@ -17,6 +17,7 @@ OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
           -4: "sampler status set", -5: "no CUDA device"}
 SIGMA1, SIGMA2, SIGMA3 = 0, 1, 2
+OBJ_MPK, OBJ_MSK, OBJ_CT, OBJ_SKY, OBJ_DY = 1, 2, 3, 4, 5
 Q = (16760833, 2147352577, 2130706433)
 
 _lib = None
@@ -100,6 +101,9 @@ def lib():
             "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
             "cufe_sampler_call_search": [i],
+            "cufe_serialized_bytes": [vp, i, i],
+            "cufe_serialize": [vp, i, i, vp, vp, vp],
+            "cufe_deserialize": [vp, i, i, vp, C.c_size_t, vp, vp],
             "cufe_dropin_configure": [i, i, i],
             "cufe_dropin_status": [],
             "rlwe_sife_setup_gpu": [vp, vp, vp, vp, vp],
@@ -112,6 +116,7 @@ def lib():
             f.argtypes = args
             f.restype = None if name.startswith("rlwe_sife_") else C.c_int
         L.cufe_sampler_refills.restype = C.c_longlong
+        L.cufe_serialized_bytes.restype = C.c_longlong
         for name in ("cufe_server_encrypt", "cufe_server_keygen", "cufe_server_decrypt"):
             getattr(L, name).restype = C.c_longlong
         L.cufe_server_now.argtypes = []
@@ -312,6 +317,30 @@ class Context:
         count = dy.numel() // (3 * self.n)
         out = _dev((count, ncoeff), self.dev) if out is None else out
         _check(lib().cufe_decode(self.h, count, _ptr(dy), ncoeff, _ptr(out), _stream(stream, self.device)), "cufe_decode")
+        return out
+
+    # ---- serialization
+    def serialize(self, kind, t, stream=None):
+        """pack count objects of `kind` (OBJ_*) from device tensor t: a uint8 device tensor"""
+        import torch
+        count = t.numel() // (self._polys(kind) * self.n)
+        nbytes = lib().cufe_serialized_bytes(self.h, kind, count)
+        if nbytes < 0:
+            raise CufeError(int(nbytes), "cufe_serialized_bytes")
+        out = torch.empty(nbytes, dtype=torch.uint8, device=t.device)
+        _check(lib().cufe_serialize(self.h, kind, count, _ptr(t), _ptr(out), _stream(stream, self.device)),
+               "cufe_serialize")
+        return out
+
+    def _polys(self, kind):
+        return {OBJ_MPK: (self.l + 1) * 3, OBJ_MSK: self.l * 3, OBJ_CT: (self.l + 1) * 3, OBJ_SKY: 3, OBJ_DY: 3}[kind]
+
+    def deserialize(self, kind, buf, count, out=None, stream=None):
+        import torch
+        polys = self._polys(kind)
+        out = torch.empty((count, polys // 3, 3, self.n), dtype=torch.int32, device=buf.device) if out is None else out
+        _check(lib().cufe_deserialize(self.h, kind, count, _ptr(buf), buf.numel(), _ptr(out),
+                                      _stream(stream, self.device)), "cufe_deserialize")
         return out
 
     # ---- samplers

@@ -301,6 +301,20 @@ int cufe_ring_get_variant(const cufe_ring *h, int *fwd, int *inv) {
   return CUFE_OK;
 }
 
+long long cufe_serialized_bytes(const cufe_ctx *h, int kind, int count) {
+  if (!h) return CUFE_ERR_INVALID;
+  return cufe::serialized_bytes(h->c, kind, count);
+}
+
+int cufe_serialize(cufe_ctx *h, int kind, int count, const uint32_t *d_src, uint8_t *d_dst, void *stream) {
+  CTX_CALL(h, cufe::ctx_serialize(h->c, kind, count, d_src, d_dst, h->c.pick(stream)));
+}
+
+int cufe_deserialize(cufe_ctx *h, int kind, int count, const uint8_t *d_src, size_t src_bytes, uint32_t *d_dst,
+                     void *stream) {
+  CTX_CALL(h, cufe::ctx_deserialize(h->c, kind, count, d_src, src_bytes, d_dst, h->c.pick(stream)));
+}
+
 int cufe_sampler_call_search(int mode) {
   if (mode < 0 || mode > 1) return CUFE_ERR_INVALID;
   cufe::set_call_search(mode);

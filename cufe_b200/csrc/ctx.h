@@ -76,6 +76,10 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
 int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                         const uint32_t *d_sky, uint32_t *d_dy, cudaStream_t s);
 int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, cudaStream_t s);
+long long serialized_bytes(const Ctx &c, int kind, int count);
+int ctx_serialize(Ctx &c, int kind, int count, const uint32_t *d_src, uint8_t *d_dst, cudaStream_t s);
+int ctx_deserialize(Ctx &c, int kind, int count, const uint8_t *d_src, size_t src_bytes, uint32_t *d_dst,
+                    cudaStream_t s);
 struct SvmModel;
 int svm_create(Ctx &c, SvmModel &m, int nr_class, int lsv, const int32_t *sv, int y_signed, const int *nsv,
                const double *sv_coef, const double *rho, const int *label, const uint32_t *d_msk, cudaStream_t s);

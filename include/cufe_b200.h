@@ -166,6 +166,25 @@ int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void
  * call. */
 int cufe_sampler_call_search(int mode);
 
+/* Serialized keys and ciphertexts: a 32-byte header (magic "CUFE", version 1, kind, n, l,
+ * count, residue polynomials per object, payload bytes) and the canonical residues packed at
+ * their moduli's bit widths (24, 31, 31 bits; each polynomial padded to 32 bits): 10.75 bytes
+ * per coefficient triple instead of 12.  Device buffers, 4-byte aligned; the bytes can be
+ * copied to the host and written out as they are.  No counterpart in the reference, which
+ * keeps keys and ciphertexts only as C arrays in memory. */
+#define CUFE_OBJ_MPK 1 /* [count][l+1][3][n] */
+#define CUFE_OBJ_MSK 2 /* [count][l][3][n] */
+#define CUFE_OBJ_CT 3  /* [count][l+1][3][n] */
+#define CUFE_OBJ_SKY 4 /* [count][3][n] */
+#define CUFE_OBJ_DY 5  /* [count][3][n] */
+long long cufe_serialized_bytes(const cufe_ctx *ctx, int kind, int count);
+/* synchronous on stream */
+int cufe_serialize(cufe_ctx *ctx, int kind, int count, const uint32_t *d_src, uint8_t *d_dst, void *stream);
+/* synchronous; CUFE_ERR_INVALID if the header does not match (kind, the context's n and l,
+ * count) or a residue is not below its modulus */
+int cufe_deserialize(cufe_ctx *ctx, int kind, int count, const uint8_t *d_src, size_t src_bytes, uint32_t *d_dst,
+                     void *stream);
+
 /* =====================================================================================
  * 2a. Encrypted linear-SVM prediction: the svm_predict5 path (svm_predict_gpu,
  *     main.c:270-390) with the support vectors' function keys derived once and resident.
