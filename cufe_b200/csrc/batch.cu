@@ -501,7 +501,7 @@ int Batch::run(cudaStream_t s) {
   for (size_t ci = 0; ci < chunks.size(); ++ci) {
     const BatchChunk &ch = chunks[ci];
     const SegDev sg2 = seg_bind(tables + ch.seg2_off, ch.count), sg3 = seg_bind(tables + ch.seg3_off, ch.count);
-    rc = sample_cpu_map_seg(1, sg2, ch.z2, rk2 + (size_t)ch.first * 60, s2o, samp, status, num_sms, s, nullptr);
+    rc = sample_cpu_map_seg(1, sg2, ch.z2, rk2 + (size_t)ch.first * 60, s2o, samp, status, num_sms, s);
     if (rc) return rc;
     for (const BatchGroup &g : ch.groups) {
       const size_t nn = (size_t)1 << g.logn;
@@ -510,7 +510,7 @@ int Batch::run(cudaStream_t s) {
       rc = ntt_fwd_shoup_launch(ctx[(int)nn]->ring.args, rh + g.rh, rhsh + g.rh, (long long)g.count * 3, s);
       if (rc) return rc;
     }
-    rc = sample_cpu_map_seg(2, sg3, ch.z3, rk3 + (size_t)ch.first * 60, f3, samp, status, num_sms, s, nullptr);
+    rc = sample_cpu_map_seg(2, sg3, ch.z3, rk3 + (size_t)ch.first * 60, f3, samp, status, num_sms, s);
     if (rc) return rc;
     for (const BatchGroup &g : ch.groups) {
       const RingArgs &ra = ctx[1 << g.logn]->ring.args;
@@ -975,7 +975,7 @@ struct Server {
       const uint8_t *seeds = d_tab + seeds_off;
       if ((rc = expand_keys_device(seeds, nullptr, 2 * ne, rk, stream))) return rc;
       if ((rc = sample_cpu_map_seg(1, seg_bind(d_tab + seg2, ne), z2, rk, s2o, samp, tenants.status, tenants.num_sms,
-                                   stream, nullptr)))
+                                   stream)))
         return rc;
       for (const BatchGroup &g : groups) {
         const size_t nn1 = (size_t)1 << g.logn;
@@ -986,7 +986,7 @@ struct Server {
           return rc;
       }
       if ((rc = sample_cpu_map_seg(2, seg_bind(d_tab + seg3, ne), z3, rk + (size_t)ne * 60, f3, samp, tenants.status,
-                                   tenants.num_sms, stream, nullptr)))
+                                   tenants.num_sms, stream)))
         return rc;
       const uint32_t *xd = reinterpret_cast<const uint32_t *>(d_tab + x_off);
       for (const BatchGroup &g : groups) {

@@ -847,7 +847,7 @@ size_t cpu_map_workspace_bytes(uint32_t nstreams, uint32_t calls, uint32_t n, in
 }
 
 int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint32_t *d_rkeys, uint32_t *d_out,
-                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
+                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s) {
   if (sig < 0 || sig > 2 || z.nstreams == 0 || z.tiles >= (1u << 31) || z.calls >= (1ull << 31) ||
       z.refills >= (1ull << 32) - (1ull << 24))
     return CUFE_ERR_INVALID;
@@ -895,14 +895,6 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
     k_walk<<<(z.nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), cstart, d_status);
   }
   CUFE_CUDA(cudaGetLastError());
-  if (out) {
-    out->cand = cand;
-    out->amask = amask;
-    out->call_start = cstart;
-    out->elocal = elocal;
-    out->tile_off = tsum;
-    out->sg = sg;
-  }
   if (d_out && z.calls) {
     ProfScope ps_sc("sample_scatter", s);
     k_scatter<<<(uint32_t)z.calls, 256, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
@@ -930,16 +922,6 @@ static int seg_uniform(uint32_t nstreams, uint32_t calls, uint32_t n, int sig, v
   return CUFE_OK;
 }
 
-int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
-                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out) {
-  SegDev sg;
-  SegSizes z;
-  void *scratch;
-  int rc = seg_uniform(nstreams, calls, n, sig, ws, s, &sg, &z, &scratch);
-  if (rc) return rc;
-  return sample_cpu_map_seg(sig, sg, z, d_rkeys, nullptr, scratch, d_status, num_sms, s, out);
-}
-
 int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
                    uint32_t *d_out, void *ws, uint32_t *d_status, int num_sms, cudaStream_t s) {
   SegDev sg;
@@ -947,7 +929,7 @@ int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t
   void *scratch;
   int rc = seg_uniform(nstreams, calls, n, sig, ws, s, &sg, &z, &scratch);
   if (rc) return rc;
-  return sample_cpu_map_seg(sig, sg, z, d_rkeys, d_out, scratch, d_status, num_sms, s, nullptr);
+  return sample_cpu_map_seg(sig, sg, z, d_rkeys, d_out, scratch, d_status, num_sms, s);
 }
 
 int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npolys, uint32_t n, uint32_t *d_out,

@@ -64,22 +64,9 @@ SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_
                        void *host_base);
 size_t seg_scratch_bytes(const SegSizes &z);
 
-// The candidate form, for consumers that gather the samples themselves: cand[g][8] signed
-// candidates and amask[g] accept bits of flattened refill g; sample j of call c of stream s
-// is the j-th accepted candidate of refills call_start[..c] .. call_start[..c+1]-1.
-struct CpuMapCandidates {
-  const int64_t *cand;
-  const uint8_t *amask;
-  const uint32_t *call_start;
-  const uint32_t *elocal, *tile_off;  // exclusive prefix of accept counts: elocal[g] + tile_off[tile]
-  SegDev sg;
-};
-// segmented run: candidates, scan, walk, and (d_out != NULL) the scatter; out (optional)
-// receives the candidate form
+// segmented run: candidates, scan, call starts and the scatter of the residues to d_out
 int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint32_t *d_rkeys, uint32_t *d_out,
-                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out);
-int sample_cpu_map_candidates(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t calls, uint32_t n,
-                              void *ws, uint32_t *d_status, int num_sms, cudaStream_t s, CpuMapCandidates *out);
+                       void *scratch, uint32_t *d_status, int num_sms, cudaStream_t s);
 
 // GPU counter mapping: polynomials poly0 .. poly0+npolys-1 of one key, residues to
 // d_out[npolys][3][n].
