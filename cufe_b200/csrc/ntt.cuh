@@ -134,10 +134,17 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_
 #pragma unroll
           for (int p = 0; p < P_; ++p) {
             if constexpr (!INV) {
+              // An output that the next stage of this pass multiplies by a twiddle (register
+              // bit half/2 set) may stay in [0, 2q): Shoup takes any input below 2^32.  The
+              // others, and every output of a pass's last stage, are reduced to [0, q).  The
+              // element multiplied here may arrive unreduced; U never does.
               const uint32_t V = shoup_mul(a[p][e2], w[g], wsh[g], q);
               const uint32_t U = a[p][e1];
-              a[p][e1] = mod_add(U, V, q);
-              a[p][e2] = mod_sub(U, V, q);
+              constexpr int nh = half >> 1;
+              const bool lazy1 = (LS + 1 < rb) && ((e1 & nh) != 0);
+              const bool lazy2 = (LS + 1 < rb) && ((e2 & nh) != 0);
+              a[p][e1] = lazy1 ? U + V : mod_add(U, V, q);
+              a[p][e2] = lazy2 ? U - V + q : mod_sub(U, V, q);
             } else {
               const uint32_t U = a[p][e1], V = a[p][e2];
               a[p][e1] = mod_add(U, V, q);
