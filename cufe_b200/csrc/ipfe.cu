@@ -150,7 +150,10 @@ int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
   }
   args.n = n;
   args.logn = logn;
-  args.pp_fwd = args.pp_inv = 1;
+  // untuned defaults: the variants that measured fastest across n on a B200 (forward: two
+  // residues per group; inverse: one residue at 40 warps per SM)
+  args.pp_fwd = 2;
+  args.pp_inv = 4;
   args.k = k;
   CUFE_CUDA(cudaSetDevice(device));
   CUFE_CUDA(cudaMalloc(&d_tab, tab.size() * 4));
@@ -172,9 +175,13 @@ namespace {
 // MODE 0 forward, 1 forward + Shoup companions into sh, 2 inverse.  data holds `rows`
 // polynomials of k residues ([row][k][n]); a thread group transforms PP residues of one
 // modulus m, rows PP*t .. PP*t+PP-1, sharing twiddles and shared-memory addresses.
-template <int LOGN, int MODE, int PP>
-__global__ void __launch_bounds__(512) k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows,
-                                             RingArgs ra) {
+// LBT, MINB: the launch bounds the registers are allocated for -- LBT threads per CTA (at
+// least the CTA's real size) and MINB CTAs per SM.  Variant 1 uses (512, 1): at most 128
+// registers; variant 2 (its CTA size, 1): up to 255, its two residues want more than 128;
+// variant 4 (256, 5): 48 registers and 40 warps per SM.
+template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1>
+__global__ void __launch_bounds__(LBT, MINB)
+    k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows, RingArgs ra) {
   using P = NttPlan<LOGN>;
   extern __shared__ uint32_t smem_u32[];
   const int th = threadIdx.x, k = ra.k;
@@ -227,21 +234,22 @@ __global__ void __launch_bounds__(512) k_ntt(uint32_t *__restrict__ data, uint32
   }
 }
 
-template <int LOGN, int MODE, int PP>
+template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1>
 int launch_ntt_pp(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long rows, cudaStream_t s) {
   using P = NttPlan<LOGN>;
   constexpr int G = ppc<LOGN>();
   const size_t smem = (size_t)G * PP * P::N * 4;
   static bool attr = false;
   if (!attr) {
-    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP, LBT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   96 * 1024));
     attr = true;
   }
   const long long groups = (rows + PP - 1) / PP * ra.k;
   const long long grid = (groups + G - 1) / G;
   if (grid <= 0) return CUFE_OK;
   ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
-  k_ntt<LOGN, MODE, PP><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra);
+  k_ntt<LOGN, MODE, PP, LBT, MINB><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -350,7 +358,9 @@ int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nre
   const long long rows = nres / ra.k;
   const int pp = MODE == 2 ? ra.pp_inv : ra.pp_fwd;
   if (pp == 3) return launch_ntt_stream<LOGN, MODE>(ra, data, sh, nres, s);
-  if (pp == 2 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2>(ra, data, sh, rows, s);
+  constexpr int nt = NttPlan<LOGN>::T * ppc<LOGN>();  // threads per CTA
+  if (pp == 2 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, 1>(ra, data, sh, rows, s);
+  if (pp == 4) return launch_ntt_pp<LOGN, MODE, 1, nt, nt <= 256 ? 5 : 2>(ra, data, sh, rows, s);
   return launch_ntt_pp<LOGN, MODE, 1>(ra, data, sh, rows, s);
 }
 
@@ -631,8 +641,8 @@ int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s) {
   // zero residues: the kernels' instruction stream does not depend on the values
   cudaError_t err = cudaMemsetAsync(buf, 0, (size_t)npoly * poly_bytes, s);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  constexpr int NV = 3;
-  float t[2 * NV] = {0, 0, 0, 0, 0, 0};
+  constexpr int NV = 4;
+  float t[2 * NV] = {0, 0, 0, 0, 0, 0, 0, 0};
   int rc = CUFE_OK;
   if (err == cudaSuccess) err = cudaEventCreate(&e0);
   if (err == cudaSuccess) err = cudaEventCreate(&e1);

@@ -315,10 +315,12 @@ int cufe_ntt_inverse(const cufe_ring *ring, uint32_t *d_data, long long npoly, v
  * one group per residue.  Variant 2: two residues of the same modulus (rows 2t and 2t+1)
  * per group, sharing twiddle loads and shared-memory addresses.  Variant 3: persistent
  * groups (a grid of one wave) that load their next residue into registers while
- * transforming the current one.  cufe_ring_tune times the three variants in both directions
- * on a scratch buffer of npoly polynomials (capped at 1 GiB, allocated and freed inside the
- * call, synchronous) and keeps the fastest per direction; ms (optional) receives
- * {fwd v1, v2, v3, inv v1, v2, v3} in milliseconds per launch.  A new ring uses variant 1.
+ * transforming the current one.  Variant 4: variant 1 compiled for 5 CTAs per SM (48
+ * registers per thread; 256-thread CTAs).  cufe_ring_tune times the four variants in both
+ * directions on a scratch buffer of npoly polynomials (capped at 1 GiB, allocated and freed
+ * inside the call, synchronous) and keeps the fastest per direction; ms (optional) receives
+ * {fwd v1, v2, v3, v4, inv v1, v2, v3, v4} in milliseconds per launch.  A new ring uses
+ * variant 2 forward and 4 inverse (the fastest across n when measured).
  * No counterpart in the reference. */
 int cufe_ring_tune(cufe_ring *ring, long long npoly, float *ms, void *stream);
 int cufe_ring_set_variant(cufe_ring *ring, int fwd, int inv);
