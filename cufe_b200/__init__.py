@@ -404,11 +404,11 @@ class Ring:
         return data
 
     def tune(self, npoly, stream=None):
-        """time the four kernel variants in both directions on npoly scratch polynomials and
-        keep the fastest; returns {"fwd": [ms v1..v4], "inv": [...], "variant": (fwd, inv)}"""
-        ms = np.zeros(8, np.float32)
+        """time the six kernel variants in both directions on npoly scratch polynomials and
+        keep the fastest; returns {"fwd": [ms v1..v6], "inv": [...], "variant": (fwd, inv)}"""
+        ms = np.zeros(12, np.float32)
         _check(lib().cufe_ring_tune(self.h, npoly, ms.ctypes.data, _stream(stream, self.device)), "cufe_ring_tune")
-        return {"fwd": [float(x) for x in ms[:4]], "inv": [float(x) for x in ms[4:]], "variant": self.variant}
+        return {"fwd": [float(x) for x in ms[:6]], "inv": [float(x) for x in ms[6:]], "variant": self.variant}
 
     @property
     def variant(self):

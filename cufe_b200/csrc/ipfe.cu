@@ -150,10 +150,9 @@ int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
   }
   args.n = n;
   args.logn = logn;
-  // untuned defaults: the variants that measured fastest across n on a B200 (forward: two
-  // residues per group; inverse: one residue at 40 warps per SM)
-  args.pp_fwd = 2;
-  args.pp_inv = 4;
+  // untuned defaults: the variants that measured fastest on a B200 (two residues per group at
+  // 4 CTAs per SM up to n = 4096; one residue at 40 warps per SM for n = 8192's 512-thread CTAs)
+  args.pp_fwd = args.pp_inv = logn >= 13 ? 4 : 6;
   args.k = k;
   CUFE_CUDA(cudaSetDevice(device));
   CUFE_CUDA(cudaMalloc(&d_tab, tab.size() * 4));
@@ -178,7 +177,8 @@ namespace {
 // LBT, MINB: the launch bounds the registers are allocated for -- LBT threads per CTA (at
 // least the CTA's real size) and MINB CTAs per SM.  Variant 1 uses (512, 1): at most 128
 // registers; variant 2 (its CTA size, 1): up to 255, its two residues want more than 128;
-// variant 4 (256, 5): 48 registers and 40 warps per SM.
+// variant 4 (256, 5): 48 registers and 40 warps per SM; variants 5 and 6: two residues at
+// 3 or 4 CTAs per SM (80 or 64 registers).
 template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1>
 __global__ void __launch_bounds__(LBT, MINB)
     k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows, RingArgs ra) {
@@ -361,6 +361,8 @@ int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nre
   constexpr int nt = NttPlan<LOGN>::T * ppc<LOGN>();  // threads per CTA
   if (pp == 2 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, 1>(ra, data, sh, rows, s);
   if (pp == 4) return launch_ntt_pp<LOGN, MODE, 1, nt, nt <= 256 ? 5 : 2>(ra, data, sh, rows, s);
+  if (pp == 5 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, nt <= 256 ? 3 : 1>(ra, data, sh, rows, s);
+  if (pp == 6 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, nt <= 256 ? 4 : 1>(ra, data, sh, rows, s);
   return launch_ntt_pp<LOGN, MODE, 1>(ra, data, sh, rows, s);
 }
 
@@ -641,8 +643,8 @@ int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s) {
   // zero residues: the kernels' instruction stream does not depend on the values
   cudaError_t err = cudaMemsetAsync(buf, 0, (size_t)npoly * poly_bytes, s);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  constexpr int NV = 4;
-  float t[2 * NV] = {0, 0, 0, 0, 0, 0, 0, 0};
+  constexpr int NV = 6;
+  float t[2 * NV] = {};
   int rc = CUFE_OK;
   if (err == cudaSuccess) err = cudaEventCreate(&e0);
   if (err == cudaSuccess) err = cudaEventCreate(&e1);

@@ -316,11 +316,12 @@ int cufe_ntt_inverse(const cufe_ring *ring, uint32_t *d_data, long long npoly, v
  * per group, sharing twiddle loads and shared-memory addresses.  Variant 3: persistent
  * groups (a grid of one wave) that load their next residue into registers while
  * transforming the current one.  Variant 4: variant 1 compiled for 5 CTAs per SM (48
- * registers per thread; 256-thread CTAs).  cufe_ring_tune times the four variants in both
- * directions on a scratch buffer of npoly polynomials (capped at 1 GiB, allocated and freed
- * inside the call, synchronous) and keeps the fastest per direction; ms (optional) receives
- * {fwd v1, v2, v3, v4, inv v1, v2, v3, v4} in milliseconds per launch.  A new ring uses
- * variant 2 forward and 4 inverse (the fastest across n when measured).
+ * registers per thread; 256-thread CTAs).  Variants 5 and 6: variant 2 compiled for 3 or 4
+ * CTAs per SM.  cufe_ring_tune times the six variants in both directions on a scratch buffer
+ * of npoly polynomials (capped at 1 GiB, allocated and freed inside the call, synchronous)
+ * and keeps the fastest per direction; ms (optional) receives {fwd v1..v6, inv v1..v6} in
+ * milliseconds per launch.  A new ring uses variant 6 (n <= 4096) or 4 (n = 8192), the
+ * fastest when measured on a B200.
  * No counterpart in the reference. */
 int cufe_ring_tune(cufe_ring *ring, long long npoly, float *ms, void *stream);
 int cufe_ring_set_variant(cufe_ring *ring, int fwd, int inv);
