@@ -305,8 +305,12 @@ def gpu_arm(args):
     scratch = torch.empty((B, N), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(local)
 
+    def first(k):
+        """first encryption of step k on this rank: ranks take disjoint batches"""
+        return ((k * world + rank) % nb) * B
+
     def step(k, out):
-        b0 = (k % nb) * B
+        b0 = first(k)
         ctx.encrypt(x_dev[b0:b0 + B], mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
         ctx.decrypt(ct, y_dev, sky, y_signed=True, dy=dy)
         ctx.decode(dy, out=out)
@@ -342,7 +346,7 @@ def gpu_arm(args):
     got = cf.u32(res[:, :, 0]).astype(np.int64)
     p = ctx.p
     got = np.where(got > p // 2, got - p, got)
-    ids = np.array([((warm + k) % nb) * B + j for k in range(steps) for j in range(B)]).reshape(steps, B)
+    ids = np.array([first(warm + k) + j for k in range(steps) for j in range(B)]).reshape(steps, B)
     exp = x[ids].astype(np.int64) @ y[0].astype(np.int64)
     bit_exact = bool((got == exp).all())
     ips = steps * B * world / (ms / 1000.0)
@@ -373,7 +377,7 @@ def gpu_arm(args):
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g0.record(stream)
     for k in range(steps):
-        b0 = ((warm + k) % nb) * B
+        b0 = first(warm + k)
         ctx.encrypt(x_dev[b0:b0 + B], mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
         ctx.decrypt_coef0(ct, y_dev, sky, y_signed=True, out=r0[k])
     g1.record(stream)
@@ -395,7 +399,7 @@ def gpu_arm(args):
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for k in range(steps):
-        b0 = ((warm + k) % nb) * B
+        b0 = first(warm + k)
         xd.copy_(xh[b0:b0 + B], non_blocking=True)
         ctx.encrypt(xd, mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
         ctx.decrypt(ct, y_dev, sky, y_signed=True, dy=dy)
