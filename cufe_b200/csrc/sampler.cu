@@ -812,14 +812,14 @@ SegSizes seg_fill_host(int sig, uint32_t S, const uint32_t *calls, const uint32_
   hr[S] = z.refills;
   ht[S] = z.tiles;
   hco[S] = z.calls;
-  z.doubling = seg_auto_doubling(z.refills);
+  z.doubling = seg_auto_doubling(z.refills, z.max_calls);
   return z;
 }
 
 static SegSizes seg_uniform_sizes(uint32_t S, uint32_t calls, uint32_t n, int sig) {
   const uint32_t R = cpu_map_refills(calls, n, sig);
   return SegSizes{S, (uint64_t)S * R, S * ((R + kScanTile - 1) / kScanTile), (uint64_t)S * calls, calls,
-                  seg_auto_doubling((uint64_t)S * R)};
+                  seg_auto_doubling((uint64_t)S * R, calls)};
 }
 
 static int g_call_search = 0;
@@ -833,7 +833,14 @@ static int doubling_levels(uint32_t max_calls) {
   while (k < 31 && (1u << k) <= max_calls) ++k;
   return k;  // bit_length(max_calls), at least 1
 }
-bool seg_auto_doubling(uint64_t refills) { return g_call_search != 1 && refills <= kDoublingMaxRefills; }
+// Doubling costs about 3.2 ps per refill per table level (memory-bound gathers); the walk
+// about 0.7 us per call of its longest stream (serial dependent loads), both measured on a
+// B200.  Doubling is chosen when it is the cheaper of the two and its tables stay below 32 Mi
+// refills.
+bool seg_auto_doubling(uint64_t refills, uint32_t max_calls) {
+  if (g_call_search == 1 || refills > kDoublingMaxRefills) return false;
+  return refills * (uint64_t)doubling_levels(max_calls) <= (uint64_t)max_calls * 200000u;
+}
 
 size_t seg_scratch_bytes(const SegSizes &z) {
   size_t b = align256(z.refills * 64) + align256(z.refills) + align256(z.refills * 4) + align256((size_t)z.tiles * 4) +

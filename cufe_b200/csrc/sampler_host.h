@@ -46,12 +46,14 @@ struct SegSizes {
   bool doubling;       // call starts by pointer doubling (its tables are part of the scratch)
 };
 // How the call starts of the CPU mapping are found.  Pointer doubling is parallel over
-// refills and calls but needs bit_length(max_calls) words per refill of scratch, so it is
-// chosen up to 32 Mi refills; the serial walk (one warp per stream) otherwise, or always
-// after set_call_search(1).  The choice is fixed in SegSizes when a scratch is sized.
+// refills and calls but costs bit_length(max_calls) table passes over all refills (and as
+// many words of scratch per refill); the serial walk (one warp per stream) costs a dependent
+// search per call.  Doubling is chosen when it is estimated cheaper and stays below 32 Mi
+// refills; set_call_search(1) forces the walk.  The choice is fixed in SegSizes when a
+// scratch is sized.
 void set_call_search(int mode);
 int get_call_search();
-bool seg_auto_doubling(uint64_t refills);
+bool seg_auto_doubling(uint64_t refills, uint32_t max_calls);
 struct SegLayout {
   size_t n, calls, toff, roff, coff, ooff, bytes;
 };
