@@ -18,6 +18,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
           -4: "sampler status set", -5: "no CUDA device"}
 SIGMA1, SIGMA2, SIGMA3 = 0, 1, 2
 OBJ_MPK, OBJ_MSK, OBJ_CT, OBJ_SKY, OBJ_DY = 1, 2, 3, 4, 5
+NTT_VARIANTS = 9  # CUFE_NTT_VARIANTS
 Q = (16760833, 2147352577, 2130706433)
 
 _lib = None
@@ -404,11 +405,12 @@ class Ring:
         return data
 
     def tune(self, npoly, stream=None):
-        """time the six kernel variants in both directions on npoly scratch polynomials and
-        keep the fastest; returns {"fwd": [ms v1..v6], "inv": [...], "variant": (fwd, inv)}"""
-        ms = np.zeros(12, np.float32)
+        """time the NTT_VARIANTS kernel variants in both directions on npoly scratch polynomials
+        and keep the fastest; returns {"fwd": [ms v1..], "inv": [...], "variant": (fwd, inv)}"""
+        ms = np.zeros(2 * NTT_VARIANTS, np.float32)
         _check(lib().cufe_ring_tune(self.h, npoly, ms.ctypes.data, _stream(stream, self.device)), "cufe_ring_tune")
-        return {"fwd": [float(x) for x in ms[:6]], "inv": [float(x) for x in ms[6:]], "variant": self.variant}
+        return {"fwd": [float(x) for x in ms[:NTT_VARIANTS]], "inv": [float(x) for x in ms[NTT_VARIANTS:]],
+                "variant": self.variant}
 
     @property
     def variant(self):

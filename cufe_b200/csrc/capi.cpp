@@ -288,7 +288,7 @@ int cufe_ring_tune(cufe_ring *h, long long npoly, float *ms, void *stream) {
 }
 
 int cufe_ring_set_variant(cufe_ring *h, int fwd, int inv) {
-  if (!h || fwd < 1 || fwd > 6 || inv < 1 || inv > 6) return CUFE_ERR_INVALID;
+  if (!h || fwd < 1 || fwd > CUFE_NTT_VARIANTS || inv < 1 || inv > CUFE_NTT_VARIANTS) return CUFE_ERR_INVALID;
   h->r.args.pp_fwd = fwd;
   h->r.args.pp_inv = inv;
   return CUFE_OK;

@@ -147,12 +147,13 @@ int Ring::init(int n_, int k_, const uint32_t *primes, int dev) {
     args.ninv_sh[m] = shoup_of(args.ninv[m], (uint32_t)qq);
     args.w1n[m] = (uint32_t)((uint64_t)h_ipsi[(size_t)m * n + 1] * args.ninv[m] % qq);
     args.w1n_sh[m] = shoup_of(args.w1n[m], (uint32_t)qq);
+    args.qr[m] = (uint32_t)((1ull << 32) / qq);
   }
   args.n = n;
   args.logn = logn;
-  // untuned defaults: the variants that measured fastest on a B200 (two residues per group at
-  // 4 CTAs per SM up to n = 4096; one residue at 40 warps per SM for n = 8192's 512-thread CTAs)
-  args.pp_fwd = args.pp_inv = logn >= 13 ? 4 : 6;
+  // untuned default: the variant that measured fastest on a B200 for every n (two residues of
+  // one modulus per group at 64 registers: 4 CTAs of 256 threads or 2 of 512 per SM)
+  args.pp_fwd = args.pp_inv = 6;
   args.k = k;
   CUFE_CUDA(cudaSetDevice(device));
   CUFE_CUDA(cudaMalloc(&d_tab, tab.size() * 4));
@@ -179,17 +180,27 @@ namespace {
 // registers; variant 2 (its CTA size, 1): up to 255, its two residues want more than 128;
 // variant 4 (256, 5): 48 registers and 40 warps per SM; variants 5 and 6: two residues at
 // 3 or 4 CTAs per SM (80 or 64 registers).
-template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1>
+// the moduli one launch covers: residues r = row * k + m[i] for i < nm
+struct ModSel {
+  int nm;
+  int m[kMaxModuli];
+};
+
+// Batched transform of rows x (selected moduli) residue polynomials, PP residues of one
+// modulus per thread group.  SQ: every selected modulus is below kSmallQ (lazy butterflies);
+// the launcher runs one grid over the small moduli and one over the others.
+template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1, int LE = 4, bool SQ = false>
 __global__ void __launch_bounds__(LBT, MINB)
-    k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows, RingArgs ra) {
-  using P = NttPlan<LOGN>;
+    k_ntt(uint32_t *__restrict__ data, uint32_t *__restrict__ sh, long long rows, RingArgs ra, ModSel sel) {
+  using P = NttPlan<LOGN, LE>;
+  constexpr int E = P::E;
   extern __shared__ uint32_t smem_u32[];
-  const int th = threadIdx.x, k = ra.k;
-  const long long groups = (rows + PP - 1) / PP * k;
+  const int th = threadIdx.x, k = ra.k, nm = sel.nm;
+  const long long groups = (rows + PP - 1) / PP * nm;
   const long long gi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
   const long long gg = gi < groups ? gi : groups - 1;
-  const int m = (int)(gg % k);
-  const long long row0 = gg / k * PP;
+  const int m = sel.m[gg % nm];
+  const long long row0 = gg / nm * PP;
   const uint32_t q = ra.q[m];
   uint32_t *sm = smem_u32 + threadIdx.y * PP * P::N;
   long long res[PP];
@@ -199,59 +210,76 @@ __global__ void __launch_bounds__(LBT, MINB)
     live[p] = gi < groups && row0 + p < rows;
     res[p] = (live[p] ? row0 + p : row0) * k + m;  // a dead slot recomputes row0, stores nothing
   }
-  uint32_t a[PP][16];
+  uint32_t a[PP][E];
   if (MODE != 2) {
 #pragma unroll
     for (int p = 0; p < PP; ++p) {
       const uint32_t *d = data + res[p] * P::N;
 #pragma unroll
-      for (int e = 0; e < 16; ++e) a[p][e] = d[P::template idx<0>(th, e)];
+      for (int e = 0; e < E; ++e) a[p][e] = d[P::template idx<0>(th, e)];
     }
-    ntt_fwd_core<LOGN, PP>(a, sm, th, q, ra.psi2 + (size_t)m * P::N);
+    ntt_fwd_core<LOGN, PP, LE, SQ>(a, sm, th, q, ra.psi2 + (size_t)m * P::N, ra.qr[m]);
 #pragma unroll
     for (int p = 0; p < PP; ++p) {
       if (!live[p]) continue;
-      store16(data + res[p] * P::N + th * 16, a[p]);
+      store_vec(data + res[p] * P::N + th * E, a[p]);
       if (MODE == 1) {
-        uint32_t b[16];
+        uint32_t b[E];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) b[e] = (uint32_t)(((uint64_t)a[p][e] << 32) / q);
-        store16(sh + res[p] * P::N + th * 16, b);
+        for (int e = 0; e < E; ++e) b[e] = (uint32_t)(((uint64_t)a[p][e] << 32) / q);
+        store_vec(sh + res[p] * P::N + th * E, b);
       }
     }
   } else {
 #pragma unroll
-    for (int p = 0; p < PP; ++p) load16(data + res[p] * P::N + th * 16, a[p]);
-    ntt_inv_core<LOGN, PP>(a, sm, th, q, ra.ipsi2 + (size_t)m * P::N, ra.ninv[m], ra.ninv_sh[m], ra.w1n[m],
-                           ra.w1n_sh[m]);
+    for (int p = 0; p < PP; ++p) load_vec(data + res[p] * P::N + th * E, a[p]);
+    ntt_inv_core<LOGN, PP, LE, SQ>(a, sm, th, q, ra.ipsi2 + (size_t)m * P::N, ra.ninv[m], ra.ninv_sh[m],
+                                   ra.w1n[m], ra.w1n_sh[m]);
 #pragma unroll
     for (int p = 0; p < PP; ++p) {
       if (!live[p]) continue;
       uint32_t *d = data + res[p] * P::N;
 #pragma unroll
-      for (int e = 0; e < 16; ++e) d[P::template idx<0>(th, e)] = a[p][e];
+      for (int e = 0; e < E; ++e) d[P::template idx<0>(th, e)] = a[p][e];
     }
   }
 }
 
-template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1>
-int launch_ntt_pp(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long rows, cudaStream_t s) {
-  using P = NttPlan<LOGN>;
-  constexpr int G = ppc<LOGN>();
+template <int LOGN, int MODE, int PP, int LBT, int MINB, int LE, bool SQ>
+int launch_ntt_sel(const RingArgs &ra, const ModSel &sel, uint32_t *data, uint32_t *sh, long long rows,
+                   cudaStream_t s) {
+  using P = NttPlan<LOGN, LE>;
+  constexpr int G = ppc<LOGN, LE>();
   const size_t smem = (size_t)G * PP * P::N * 4;
   static bool attr = false;
   if (!attr) {
-    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP, LBT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   96 * 1024));
+    CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP, LBT, MINB, LE, SQ>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     attr = true;
   }
-  const long long groups = (rows + PP - 1) / PP * ra.k;
+  const long long groups = (rows + PP - 1) / PP * sel.nm;
   const long long grid = (groups + G - 1) / G;
   if (grid <= 0) return CUFE_OK;
-  ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
-  k_ntt<LOGN, MODE, PP, LBT, MINB><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra);
+  k_ntt<LOGN, MODE, PP, LBT, MINB, LE, SQ><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra, sel);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
+}
+
+// one grid over the moduli below kSmallQ (lazy butterflies), one over the rest
+template <int LOGN, int MODE, int PP, int LBT = 512, int MINB = 1, int LE = 4>
+int launch_ntt_pp(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long rows, cudaStream_t s) {
+  ModSel small{0, {}}, large{0, {}};
+  for (int m = 0; m < ra.k; ++m) {
+    if (ra.q[m] < kSmallQ)
+      small.m[small.nm++] = m;
+    else
+      large.m[large.nm++] = m;
+  }
+  ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
+  int rc = CUFE_OK;
+  if (small.nm) rc = launch_ntt_sel<LOGN, MODE, PP, LBT, MINB, LE, true>(ra, small, data, sh, rows, s);
+  if (!rc && large.nm) rc = launch_ntt_sel<LOGN, MODE, PP, LBT, MINB, LE, false>(ra, large, data, sh, rows, s);
+  return rc;
 }
 
 // Persistent form: each thread group walks residues r, r + stride, ... and issues the global
@@ -362,7 +390,17 @@ int launch_ntt_t(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nre
   if (pp == 2 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, 1>(ra, data, sh, rows, s);
   if (pp == 4) return launch_ntt_pp<LOGN, MODE, 1, nt, nt <= 256 ? 5 : 2>(ra, data, sh, rows, s);
   if (pp == 5 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, nt <= 256 ? 3 : 1>(ra, data, sh, rows, s);
-  if (pp == 6 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, nt <= 256 ? 4 : 1>(ra, data, sh, rows, s);
+  if (pp == 6 && rows >= 2) return launch_ntt_pp<LOGN, MODE, 2, nt, nt <= 256 ? 4 : 2>(ra, data, sh, rows, s);
+  // radix 32 and 64: 32 or 64 coefficients per thread, fewer passes and exchanges
+  if constexpr (LOGN >= 10) {
+    constexpr int nt5 = NttPlan<LOGN, 5>::T * ppc<LOGN, 5>();
+    if (pp == 7) return launch_ntt_pp<LOGN, MODE, 1, nt5, 2, 5>(ra, data, sh, rows, s);
+    if (pp == 8) return launch_ntt_pp<LOGN, MODE, 1, nt5, 3, 5>(ra, data, sh, rows, s);
+  }
+  if constexpr (LOGN >= 11) {
+    constexpr int nt6 = NttPlan<LOGN, 6>::T * ppc<LOGN, 6>();
+    if (pp == 9) return launch_ntt_pp<LOGN, MODE, 1, nt6, 2, 6>(ra, data, sh, rows, s);
+  }
   return launch_ntt_pp<LOGN, MODE, 1>(ra, data, sh, rows, s);
 }
 
@@ -643,7 +681,7 @@ int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s) {
   // zero residues: the kernels' instruction stream does not depend on the values
   cudaError_t err = cudaMemsetAsync(buf, 0, (size_t)npoly * poly_bytes, s);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  constexpr int NV = 6;
+  constexpr int NV = CUFE_NTT_VARIANTS;
   float t[2 * NV] = {};
   int rc = CUFE_OK;
   if (err == cudaSuccess) err = cudaEventCreate(&e0);

@@ -5,32 +5,36 @@
 // in, natural out) including the factor n^-1.  Any exact implementation of this linear map
 // gives the reference's values after canonical reduction, so the loop order is free.
 //
-// B200 design: n/16 threads per residue polynomial, 16 coefficients per thread held in
-// registers.  The log2(n) butterfly stages are grouped into passes of up to 4 stages
-// (radix 16); a pass touches only the 16 coefficients of a thread, and consecutive passes
+// B200 design: n/E threads per residue polynomial, E = 2^LE coefficients per thread held in
+// registers (E = 16 everywhere; the batched transform kernel also has E = 32 and 64 forms,
+// picked by the ring's tuner).  The log2(n) butterfly stages are grouped into passes of up
+// to LE stages (radix E); a pass touches only the E coefficients of a thread, and consecutive passes
 // exchange coefficients through shared memory (one __syncthreads per exchange) with an
-// XOR swizzle (j ^ ((j >> 4) & 31)) that keeps every exchange pattern of these plans free
-// of bank conflicts without padding.  The smaller pass (log2(n) mod 4 stages) comes first so that the strided
-// passes are the early ones, whose warps touch 32 consecutive words.  Twiddles use
-// Shoup's precomputed quotient (1 mul.hi + 2 mul.lo per product) and residues stay
-// canonical in [0, q), q < 2^31.  The inverse folds n^-1 into its last stage.
+// XOR swizzle (j ^ ((j >> s) & 31), s = 4 for radix 16 and LE otherwise) that keeps every
+// exchange pattern of these plans free of bank conflicts without padding.  The smaller pass
+// (log2(n) mod LE stages) comes first so that the strided passes are the early ones, whose
+// warps touch 32 consecutive words.  Twiddles use Shoup's precomputed quotient (1 mul.hi +
+// 2 mul.lo per product) and residues stay canonical in [0, q), q < 2^31, between kernels.
+// The inverse folds n^-1 into its last stage.
 #pragma once
 #include "cufe_internal.cuh"
 
 namespace cufe {
 
-template <int LOGN>
+template <int LOGN, int LE = 4>
 struct NttPlan {
+  static constexpr int E = 1 << LE;  // coefficients per thread (radix of the full passes)
   static constexpr int N = 1 << LOGN;
-  static constexpr int T = N / 16;  // threads per residue polynomial
-  static constexpr int NP = (LOGN + 3) / 4;
-  static constexpr int R0 = LOGN - 4 * (NP - 1);
+  static constexpr int T = N / E;  // threads per residue polynomial
+  static constexpr int NP = (LOGN + LE - 1) / LE;
+  static constexpr int R0 = LOGN - LE * (NP - 1);
   static constexpr int SMEM_WORDS = N;
-  __host__ __device__ static constexpr int radix_bits(int p) { return p == 0 ? R0 : 4; }
-  __host__ __device__ static constexpr int first_stage(int p) { return p == 0 ? 0 : R0 + 4 * (p - 1); }
+  __host__ __device__ static constexpr int radix_bits(int p) { return p == 0 ? R0 : LE; }
+  __host__ __device__ static constexpr int first_stage(int p) { return p == 0 ? 0 : R0 + LE * (p - 1); }
   // coefficient index held in register e by thread th during pass PASS.  The bits that come
   // from th and the bits that come from e are disjoint, so idx = idx_th(th) + idx_e(e), the
-  // second a compile-time constant (an immediate offset in every load and store).
+  // second a compile-time constant (an immediate offset in every load and store).  A pass
+  // of rb < LE stages runs E >> rb butterfly blocks per thread ("virtual threads" v*T + th).
   template <int PASS>
   __device__ __forceinline__ static int idx_th(int th) {
     constexpr int rb = radix_bits(PASS), s0 = first_stage(PASS);
@@ -47,7 +51,10 @@ struct NttPlan {
   __device__ __forceinline__ static int idx(int th, int e) {
     return idx_th<PASS>(th) + idx_e<PASS>(e);
   }
-  __host__ __device__ static constexpr int swz(int j) { return j ^ ((j >> 4) & 31); }
+  // XOR swizzle: bits LE..LE+4 of the index folded into the bank bits.  The lanes of a warp
+  // cover index bits 0..4 in the early passes and bits LE..LE+4 in the last one; the fold
+  // keeps both (and, for LE = 4, the middle pass's bits 0..3 + 8) conflict-free.
+  __host__ __device__ static constexpr int swz(int j) { return j ^ ((j >> (LE == 4 ? 4 : LE)) & 31); }
 };
 
 // P residue polynomials per thread group (same modulus, shared twiddles and addresses):
@@ -55,12 +62,12 @@ struct NttPlan {
 // The swizzle is linear over XOR and idx_th / idx_e have disjoint bits, so the swizzled
 // address of register e is swz(idx_th(th)) ^ swz(idx_e(e)): one per-thread base and one XOR
 // with a constant per access.
-template <int LOGN, int FROM, int TO, int P_>
-__device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][16], uint32_t *sm, int th) {
-  using P = NttPlan<LOGN>;
+template <int LOGN, int FROM, int TO, int P_, int LE, int E>
+__device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][E], uint32_t *sm, int th) {
+  using P = NttPlan<LOGN, LE>;
   const int wb = P::swz(P::template idx_th<FROM>(th));
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
+  for (int e = 0; e < E; ++e) {
     const int j = wb ^ P::swz(P::template idx_e<FROM>(e));
 #pragma unroll
     for (int p = 0; p < P_; ++p) sm[p * P::N + j] = a[p][e];
@@ -68,12 +75,15 @@ __device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][16], uint32_t *sm
   __syncthreads();
   const int rbase = P::swz(P::template idx_th<TO>(th));
 #pragma unroll
-  for (int e = 0; e < 16; ++e) {
+  for (int e = 0; e < E; ++e) {
     const int j = rbase ^ P::swz(P::template idx_e<TO>(e));
 #pragma unroll
     for (int p = 0; p < P_; ++p) a[p][e] = sm[p * P::N + j];
   }
 }
+
+// moduli below this take the small-modulus butterflies (SQ) where a kernel offers them
+constexpr uint32_t kSmallQ = 1u << 27;
 
 struct InvScale {
   uint32_t ninv, ninv_sh, w1n, w1n_sh;
@@ -103,12 +113,15 @@ __device__ __forceinline__ void load_twiddles(const uint2 *__restrict__ tw, int 
 
 // stage LS of pass PASS (CT stage s = first_stage(PASS) + LS; the inverse runs the same
 // butterfly positions with Gentleman-Sande butterflies and psi^-1 twiddles)
-template <int LOGN, int PASS, int LS, bool INV, int P_>
-__device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *__restrict__ tw,
+// SQ (small modulus, q < kSmallQ): the forward keeps every value unreduced -- a stage adds
+// at most 2q to the bound, so canonical inputs stay below (2 log2(n) + 1) q < 2^32 -- and is
+// reduced once after the last stage; the inverse keeps values in [0, 2q) (4q < 2^32).
+template <int LOGN, int PASS, int LS, bool INV, int P_, int LE, bool SQ, int E>
+__device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][E], int th, uint32_t q, const uint2 *__restrict__ tw,
                                           const InvScale &sc) {
-  using P = NttPlan<LOGN>;
+  using P = NttPlan<LOGN, LE>;
   constexpr int rb = P::radix_bits(PASS), s0 = P::first_stage(PASS), plo = LOGN - s0 - rb;
-  constexpr int s = s0 + LS, half = 1 << (rb - 1 - LS), nv = 16 >> rb, ng = 1 << LS;
+  constexpr int s = s0 + LS, half = 1 << (rb - 1 - LS), nv = E >> rb, ng = 1 << LS;
 #pragma unroll
   for (int v = 0; v < nv; ++v) {
     const int H = (v * P::T + th) >> plo;
@@ -120,7 +133,7 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_
         for (int p = 0; p < P_; ++p) {
           const uint32_t U = a[p][e1], V = a[p][e2];
           a[p][e1] = shoup_mul(U + V, sc.ninv, sc.ninv_sh, q);
-          a[p][e2] = shoup_mul(U - V + q, sc.w1n, sc.w1n_sh, q);
+          a[p][e2] = shoup_mul(U - V + (SQ ? 2 * q : q), sc.w1n, sc.w1n_sh, q);
         }
       }
     } else {
@@ -133,7 +146,16 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_
           const int e1 = (v << rb) + g * 2 * half + b, e2 = e1 + half;
 #pragma unroll
           for (int p = 0; p < P_; ++p) {
-            if constexpr (!INV) {
+            if constexpr (!INV && SQ) {
+              const uint32_t V = shoup_lazy(a[p][e2], w[g], wsh[g], q);  // [0, 2q)
+              const uint32_t U = a[p][e1];
+              a[p][e1] = U + V;
+              a[p][e2] = U - V + 2 * q;
+            } else if constexpr (INV && SQ) {
+              const uint32_t U = a[p][e1], V = a[p][e2];  // both in [0, 2q)
+              a[p][e1] = __viaddmin_u32(U, V, U + V - 2 * q);
+              a[p][e2] = shoup_lazy(U - V + 2 * q, w[g], wsh[g], q);
+            } else if constexpr (!INV) {
               // An output that the next stage of this pass multiplies by a twiddle (register
               // bit half/2 set) may stay in [0, 2q): Shoup takes any input below 2^32.  The
               // others, and every output of a pass's last stage, are reduced to [0, q).  The
@@ -157,38 +179,47 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][16], int th, uint32_
   }
 }
 
-template <int LOGN, int PASS, int LS, int P_>
-__device__ __forceinline__ void ntt_fwd_stages(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *tw) {
-  ntt_stage<LOGN, PASS, LS, false, P_>(a, th, q, tw, InvScale{});
-  if constexpr (LS + 1 < NttPlan<LOGN>::radix_bits(PASS)) ntt_fwd_stages<LOGN, PASS, LS + 1, P_>(a, th, q, tw);
+template <int LOGN, int PASS, int LS, int P_, int LE, bool SQ, int E>
+__device__ __forceinline__ void ntt_fwd_stages(uint32_t (&a)[P_][E], int th, uint32_t q, const uint2 *tw) {
+  ntt_stage<LOGN, PASS, LS, false, P_, LE, SQ>(a, th, q, tw, InvScale{});
+  if constexpr (LS + 1 < NttPlan<LOGN, LE>::radix_bits(PASS))
+    ntt_fwd_stages<LOGN, PASS, LS + 1, P_, LE, SQ>(a, th, q, tw);
 }
-template <int LOGN, int PASS, int P_>
-__device__ __forceinline__ void ntt_fwd_passes(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+template <int LOGN, int PASS, int P_, int LE, bool SQ, int E>
+__device__ __forceinline__ void ntt_fwd_passes(uint32_t (&a)[P_][E], uint32_t *sm, int th, uint32_t q,
                                                const uint2 *tw) {
-  if constexpr (PASS > 0) ntt_exchange<LOGN, PASS - 1, PASS, P_>(a, sm, th);
-  ntt_fwd_stages<LOGN, PASS, 0, P_>(a, th, q, tw);
-  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_fwd_passes<LOGN, PASS + 1, P_>(a, sm, th, q, tw);
+  if constexpr (PASS > 0) ntt_exchange<LOGN, PASS - 1, PASS, P_, LE>(a, sm, th);
+  ntt_fwd_stages<LOGN, PASS, 0, P_, LE, SQ>(a, th, q, tw);
+  if constexpr (PASS + 1 < NttPlan<LOGN, LE>::NP) ntt_fwd_passes<LOGN, PASS + 1, P_, LE, SQ>(a, sm, th, q, tw);
 }
-template <int LOGN, int PASS, int LS, int P_>
-__device__ __forceinline__ void ntt_inv_stages(uint32_t (&a)[P_][16], int th, uint32_t q, const uint2 *tw,
+template <int LOGN, int PASS, int LS, int P_, int LE, bool SQ, int E>
+__device__ __forceinline__ void ntt_inv_stages(uint32_t (&a)[P_][E], int th, uint32_t q, const uint2 *tw,
                                                const InvScale &sc) {
-  ntt_stage<LOGN, PASS, LS, true, P_>(a, th, q, tw, sc);
-  if constexpr (LS > 0) ntt_inv_stages<LOGN, PASS, LS - 1, P_>(a, th, q, tw, sc);
+  ntt_stage<LOGN, PASS, LS, true, P_, LE, SQ>(a, th, q, tw, sc);
+  if constexpr (LS > 0) ntt_inv_stages<LOGN, PASS, LS - 1, P_, LE, SQ>(a, th, q, tw, sc);
 }
-template <int LOGN, int PASS, int P_>
-__device__ __forceinline__ void ntt_inv_passes(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+template <int LOGN, int PASS, int P_, int LE, bool SQ, int E>
+__device__ __forceinline__ void ntt_inv_passes(uint32_t (&a)[P_][E], uint32_t *sm, int th, uint32_t q,
                                                const uint2 *tw, const InvScale &sc) {
-  if constexpr (PASS + 1 < NttPlan<LOGN>::NP) ntt_exchange<LOGN, PASS + 1, PASS, P_>(a, sm, th);
-  ntt_inv_stages<LOGN, PASS, NttPlan<LOGN>::radix_bits(PASS) - 1, P_>(a, th, q, tw, sc);
-  if constexpr (PASS > 0) ntt_inv_passes<LOGN, PASS - 1, P_>(a, sm, th, q, tw, sc);
+  if constexpr (PASS + 1 < NttPlan<LOGN, LE>::NP) ntt_exchange<LOGN, PASS + 1, PASS, P_, LE>(a, sm, th);
+  ntt_inv_stages<LOGN, PASS, NttPlan<LOGN, LE>::radix_bits(PASS) - 1, P_, LE, SQ>(a, th, q, tw, sc);
+  if constexpr (PASS > 0) ntt_inv_passes<LOGN, PASS - 1, P_, LE, SQ>(a, sm, th, q, tw, sc);
 }
 
-// Registers a[p][] hold the pass-0 layout on entry and the last-pass layout (16 consecutive
-// coefficients th*16 .. th*16+15) on exit.  sm: P_ x SMEM_WORDS scratch for this group.
-template <int LOGN, int P_>
-__device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
-                                             const uint2 *__restrict__ psi2) {
-  ntt_fwd_passes<LOGN, 0, P_>(a, sm, th, q, psi2);
+// Registers a[p][] hold the pass-0 layout on entry and the last-pass layout (E consecutive
+// coefficients th*E .. th*E+E-1) on exit.  sm: P_ x SMEM_WORDS scratch for this group.
+template <int LOGN, int P_, int LE = 4, bool SQ = false, int E>
+__device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[P_][E], uint32_t *sm, int th, uint32_t q,
+                                             const uint2 *__restrict__ psi2, uint32_t qr = 0) {
+  static_assert(E == (1 << LE), "register block size");
+  static_assert(!SQ || (2 * LOGN + 1) * (uint64_t)kSmallQ <= (1ull << 32), "small-modulus bound");
+  ntt_fwd_passes<LOGN, 0, P_, LE, SQ>(a, sm, th, q, psi2);
+  if constexpr (SQ) {  // x < (2 log2(n) + 1) q: x - floor(x qr / 2^32) q is in [0, 2q)
+#pragma unroll
+    for (int p = 0; p < P_; ++p)
+#pragma unroll
+      for (int e = 0; e < E; ++e) a[p][e] = mod_red1(a[p][e] - __umulhi(a[p][e], qr) * q, q);
+  }
 }
 template <int LOGN>
 __device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,
@@ -196,13 +227,15 @@ __device__ __forceinline__ void ntt_fwd_core(uint32_t (&a)[16], uint32_t *sm, in
   ntt_fwd_core<LOGN, 1>(reinterpret_cast<uint32_t(&)[1][16]>(a), sm, th, q, psi2);
 }
 
-// Registers hold the last-pass layout (16 consecutive coefficients) on entry and the
+// Registers hold the last-pass layout (E consecutive coefficients) on entry and the
 // pass-0 layout on exit.  Inputs must be canonical residues.
-template <int LOGN, int P_>
-__device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[P_][16], uint32_t *sm, int th, uint32_t q,
+template <int LOGN, int P_, int LE = 4, bool SQ = false, int E>
+__device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[P_][E], uint32_t *sm, int th, uint32_t q,
                                              const uint2 *__restrict__ ipsi2, uint32_t ninv, uint32_t ninv_sh,
                                              uint32_t w1n, uint32_t w1n_sh) {
-  ntt_inv_passes<LOGN, NttPlan<LOGN>::NP - 1, P_>(a, sm, th, q, ipsi2, InvScale{ninv, ninv_sh, w1n, w1n_sh});
+  static_assert(E == (1 << LE), "register block size");
+  ntt_inv_passes<LOGN, NttPlan<LOGN, LE>::NP - 1, P_, LE, SQ>(a, sm, th, q, ipsi2,
+                                                                InvScale{ninv, ninv_sh, w1n, w1n_sh});
 }
 template <int LOGN>
 __device__ __forceinline__ void ntt_inv_core(uint32_t (&a)[16], uint32_t *sm, int th, uint32_t q,

@@ -6,9 +6,9 @@
 
 namespace cufe {
 
-template <int LOGN>
+template <int LOGN, int LE = 4>
 constexpr int ppc() {  // residue polynomials per CTA (>= 256 threads per CTA)
-  return NttPlan<LOGN>::T >= 256 ? 1 : 256 / NttPlan<LOGN>::T;
+  return NttPlan<LOGN, LE>::T >= 256 ? 1 : 256 / NttPlan<LOGN, LE>::T;
 }
 
 __device__ __forceinline__ void load16(const uint32_t *p, uint32_t (&a)[16]) {
@@ -26,6 +26,25 @@ __device__ __forceinline__ void store16(uint32_t *p, const uint32_t (&a)[16]) {
   uint4 *v = reinterpret_cast<uint4 *>(p);
 #pragma unroll
   for (int i = 0; i < 4; ++i) v[i] = make_uint4(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]);
+}
+// E consecutive words (E a multiple of 4, p 16-byte aligned)
+template <int E>
+__device__ __forceinline__ void load_vec(const uint32_t *p, uint32_t (&a)[E]) {
+  const uint4 *v = reinterpret_cast<const uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < E / 4; ++i) {
+    const uint4 t = v[i];
+    a[4 * i] = t.x;
+    a[4 * i + 1] = t.y;
+    a[4 * i + 2] = t.z;
+    a[4 * i + 3] = t.w;
+  }
+}
+template <int E>
+__device__ __forceinline__ void store_vec(uint32_t *p, const uint32_t (&a)[E]) {
+  uint4 *v = reinterpret_cast<uint4 *>(p);
+#pragma unroll
+  for (int i = 0; i < E / 4; ++i) v[i] = make_uint4(a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]);
 }
 
 

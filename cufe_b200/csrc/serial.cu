@@ -22,7 +22,6 @@ namespace cufe {
 namespace {
 
 constexpr uint32_t kMagic = 0x45465543u;  // "CUFE"
-constexpr int kWidth[3] = {24, 31, 31};
 
 struct Header {
   uint32_t magic;

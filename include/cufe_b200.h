@@ -312,17 +312,25 @@ int cufe_ring_info(const cufe_ring *ring, uint32_t *primes, uint32_t *roots, uin
 int cufe_ntt_forward(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
 int cufe_ntt_inverse(const cufe_ring *ring, uint32_t *d_data, long long npoly, void *stream);
 /* Kernel variants and their tuner.  Variant 1: one residue polynomial per thread group,
- * one group per residue.  Variant 2: two residues of the same modulus (rows 2t and 2t+1)
- * per group, sharing twiddle loads and shared-memory addresses.  Variant 3: persistent
- * groups (a grid of one wave) that load their next residue into registers while
- * transforming the current one.  Variant 4: variant 1 compiled for 5 CTAs per SM (48
- * registers per thread; 256-thread CTAs).  Variants 5 and 6: variant 2 compiled for 3 or 4
- * CTAs per SM.  cufe_ring_tune times the six variants in both directions on a scratch buffer
+ * one group per residue, 16 coefficients per thread (radix-16 passes).  Variant 2: two
+ * residues of the same modulus (rows 2t and 2t+1) per group, sharing twiddle loads and
+ * shared-memory addresses.  Variant 3: persistent groups (a grid of one wave) that load
+ * their next residue into registers while transforming the current one.  Variant 4:
+ * variant 1 compiled for 5 CTAs per SM (48 registers per thread; 256-thread CTAs).
+ * Variants 5 and 6: variant 2 compiled for 3 or 4 CTAs per SM of 256 threads (n = 8192,
+ * 512-thread CTAs: 1 or 2).  Variants 7 and 8 (n >= 1024):
+ * 32 coefficients per thread (radix-32 passes: n = 1024 in 2 passes, 8192 in 3), compiled
+ * for 2 or 3 CTAs per SM.  Variant 9 (n >= 2048): 64 coefficients per thread (radix 64:
+ * n = 2048 and 4096 in 2 passes).  On smaller rings variants 7-9 run variant 1.
+ * cufe_ring_tune times the CUFE_NTT_VARIANTS variants in both directions on a scratch buffer
  * of npoly polynomials (capped at 1 GiB, allocated and freed inside the call, synchronous)
- * and keeps the fastest per direction; ms (optional) receives {fwd v1..v6, inv v1..v6} in
- * milliseconds per launch.  A new ring uses variant 6 (n <= 4096) or 4 (n = 8192), the
- * fastest when measured on a B200.
+ * and keeps the fastest per direction; ms (optional, 2 * CUFE_NTT_VARIANTS floats) receives
+ * {fwd v1..v9, inv v1..v9} in milliseconds per launch.  A new ring uses variant 6, the
+ * fastest form at every n when measured on a B200.  Every variant splits a launch into one
+ * grid over the moduli below 2^27 (lazy butterflies: no reduction in the forward until its
+ * last stage, [0, 2q) in the inverse) and one over the others.
  * No counterpart in the reference. */
+#define CUFE_NTT_VARIANTS 9
 int cufe_ring_tune(cufe_ring *ring, long long npoly, float *ms, void *stream);
 int cufe_ring_set_variant(cufe_ring *ring, int fwd, int inv);
 int cufe_ring_get_variant(const cufe_ring *ring, int *fwd, int *inv);

@@ -31,7 +31,7 @@ def ctx_small(oracle_built):
     c.close()
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", list(range(1, cf.NTT_VARIANTS + 1)))
 @pytest.mark.parametrize("n", [16, 64, 256, 1024, 2048, 4096, 8192])
 @pytest.mark.parametrize("k", [3, 6])
 def test_ntt_roundtrip_and_values(n, k, variant, rng, oracle_built):
