@@ -218,7 +218,7 @@ def algorithmic_bytes(kernel, B, refills3):
     poly = 3 * N * 4
     return {
         "sample_cand_s3": refills3 * B * 65,           # 8 x int64 candidates + accept mask
-        "sample_scatter": refills3 * B * 69 + B * L * poly,  # candidates, masks, prefixes; f_i residues
+        "sample_scatter": refills3 * B * 65 + B * L * poly,  # candidates and masks; f_i residues
         "encrypt_intt": (L + 1) * poly + B * (L * poly + (L + 1) * poly),  # mpk once, f_i, ciphertexts
         "decrypt_mac": B * (L + 1) * poly + B * poly,    # ciphertexts read, partial sums written
         "decode": B * poly + B * N * 4,

@@ -425,47 +425,84 @@ __global__ void k_starts_from_tables(const uint32_t *__restrict__ tables, int le
 
 struct ModArgs {
   uint32_t q[3];
-  uint64_t mu[3];
+  uint64_t mu[3];   // floor(2^64 / q)
+  uint32_t qr[3];   // floor(2^32 / q)
+  uint32_t c32[3];  // 2^32 mod q
 };
 
-__device__ __forceinline__ uint32_t signed_residue(int64_t s, uint32_t q, uint64_t mu) {
-  if (s >= 0) return mod_u64((uint64_t)s, mu, q);
-  const uint32_t r = mod_u64((uint64_t)(-s), mu, q);
-  return r ? q - r : 0u;
+// s mod q_j in [0, q_j).  Samples satisfy |s| < 8K < 2^33 (z = K x + y, x <= 7, y < K):
+// |s| = hi 2^32 + lo with hi <= 1, lo mod q by one multiply-high (lo - floor(lo qr / 2^32) q
+// is in [0, 2q)), plus 2^32 mod q when hi = 1; anything wider takes the 64-bit reduction.
+__device__ __forceinline__ uint32_t signed_residue(int64_t s, const ModArgs &m, int j) {
+  const uint64_t u = s >= 0 ? (uint64_t)s : (uint64_t)(-s);
+  const uint32_t q = m.q[j];
+  uint32_t r;
+  if (u < (1ull << 33)) {
+    const uint32_t lo = (uint32_t)u;
+    r = mod_red1(lo - __umulhi(lo, m.qr[j]) * q, q);
+    if (u >> 32) r = mod_add(r, m.c32[j], q);
+  } else {
+    r = mod_u64(u, m.mu[j], q);
+  }
+  return s >= 0 || r == 0 ? r : q - r;
 }
 
 // one CTA per call of the flattened call space: the accepted candidates of refills
-// [a_c, a_{c+1}) in order, as residues out[ooff[st] + c * 3n ...][3][n]
-__global__ void __launch_bounds__(256) k_scatter(const int64_t *__restrict__ cand, const uint8_t *__restrict__ amask,
-                                                 const uint32_t *__restrict__ elocal,
-                                                 const uint32_t *__restrict__ tile_off,
-                                                 const uint32_t *__restrict__ call_start, SegDev sg, ModArgs m,
-                                                 uint32_t *__restrict__ out) {
+// [a_c, a_{c+1}) in order, as residues out[ooff[st] + c * 3n ...][3][n].  Warp w of the CTA
+// takes a contiguous run of the call's refills, 32 at a time: lane L loads the accept mask of
+// refill t + L and, for k = 0..7, candidate L & 7 of refill t + 4k + L / 8 (eight coalesced
+// 256-byte loads in flight per warp).  Per k the warp ballots the accepted lanes and packs
+// them, in refill order and then candidate order (the order the reference consumes them), into
+// a per-warp staging array; then every lane reduces one staged sample and the warp writes
+// consecutive output positions.  Only the first position of each warp's run comes from the
+// prefix tables.
+constexpr int kScatterThreads = 256;
+__global__ void __launch_bounds__(kScatterThreads)
+    k_scatter(const int64_t *__restrict__ cand, const uint8_t *__restrict__ amask, const uint32_t *__restrict__ elocal,
+              const uint32_t *__restrict__ tile_off, const uint32_t *__restrict__ call_start, SegDev sg, ModArgs m,
+              uint32_t *__restrict__ out) {
+  __shared__ int64_t stage[kScatterThreads / 32][256];
   const uint32_t st = seg_find(sg.coff, sg.nstreams, blockIdx.x);
   const uint64_t cs0 = __ldg(sg.coff + st);
   const uint32_t c = (uint32_t)(blockIdx.x - cs0);
   const SegView v = seg_view(sg, st);
   const uint32_t n = __ldg(sg.n + st);
   const uint32_t *cs = call_start + cs0 + st;
-  const uint32_t a = cs[c], b = cs[c + 1];
-  if (a >= v.R) return;
-  const uint32_t base = prefix_at(elocal, tile_off, amask, v, a);
+  const uint32_t a = cs[c], b = min(cs[c + 1], v.R);
+  if (a >= b) return;
+  const uint32_t lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+  const uint32_t span = ((b - a + nw - 1) / nw + 3u) & ~3u;  // refills per warp
+  const uint32_t t0 = a + (threadIdx.x >> 5) * span;
+  if (t0 >= b) return;  // whole warps leave together; no CTA barrier follows
+  const uint32_t t1 = min(t0 + span, b);
+  uint32_t pos = prefix_at(elocal, tile_off, amask, v, t0) - prefix_at(elocal, tile_off, amask, v, a);
   uint32_t *o = out + __ldg(sg.ooff + st) + (size_t)c * 3 * n;
-  for (uint32_t t = a + threadIdx.x; t < b && t < v.R; t += blockDim.x) {
-    const uint64_t g = v.r0 + t;
-    uint32_t msk = amask[g];
-    uint32_t pos = prefix_at(elocal, tile_off, amask, v, t) - base;
-    const int64_t *cv = cand + g * 8;
-    while (msk) {
-      const int i = __ffs(msk) - 1;
-      msk &= msk - 1;
-      if (pos < n) {
-        const int64_t sv = cv[i];
+  int64_t *sw = stage[threadIdx.x >> 5];
+  const uint32_t below = (1u << lane) - 1u, ci = lane & 7u;
+  for (uint32_t t = t0; t < t1 && pos < n; t += 32) {
+    const uint32_t mk = t + lane < t1 ? __ldg(amask + v.r0 + t + lane) : 0u;
+    int64_t sv[8];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) o[j * n + pos] = signed_residue(sv, m.q[j], m.mu[j]);
-      }
-      ++pos;
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t r = t + 4 * k + (lane >> 3);
+      sv[k] = r < t1 ? __ldg(cand + (v.r0 + r) * 8 + ci) : 0;
     }
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const bool acc = (__shfl_sync(0xffffffffu, mk, 4 * k + (lane >> 3)) >> ci) & 1u;
+      const uint32_t bal = __ballot_sync(0xffffffffu, acc);
+      if (acc) sw[cnt + __popc(bal & below)] = sv[k];
+      cnt += __popc(bal);
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < cnt && pos + i < n; i += 32) {
+      const int64_t sval = sw[i];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) o[j * n + pos + i] = signed_residue(sval, m, j);
+    }
+    __syncwarp();  // the next step overwrites the staging array
+    pos += cnt;
   }
 }
 
@@ -595,7 +632,7 @@ __global__ void __launch_bounds__(256)
     const int64_t s = k ? -zs : zs;
     const uint32_t pos = 8 * t + j;
 #pragma unroll
-    for (int jj = 0; jj < 3; ++jj) o[jj * n + pos] = signed_residue(s, m.q[jj], m.mu[jj]);
+    for (int jj = 0; jj < 3; ++jj) o[jj * n + pos] = signed_residue(s, m, jj);
   }
 }
 
@@ -634,6 +671,8 @@ static ModArgs mod_args() {
     m.q[j] = kRefPrimes[j];
     unsigned __int128 one = (unsigned __int128)1 << 64;
     m.mu[j] = (uint64_t)(one / kRefPrimes[j]);
+    m.qr[j] = (uint32_t)((1ull << 32) / kRefPrimes[j]);
+    m.c32[j] = (uint32_t)((1ull << 32) % kRefPrimes[j]);
   }
   return m;
 }
@@ -904,7 +943,7 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
   CUFE_CUDA(cudaGetLastError());
   if (d_out && z.calls) {
     ProfScope ps_sc("sample_scatter", s);
-    k_scatter<<<(uint32_t)z.calls, 256, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
+    k_scatter<<<(uint32_t)z.calls, kScatterThreads, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
     CUFE_CUDA(cudaGetLastError());
   }
   return CUFE_OK;
