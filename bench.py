@@ -370,6 +370,18 @@ def gpu_arm(args):
     plain = {"value": 1000.0 * len(lat) / sum(lat), "unit": UNIT, "calls": len(lat),
              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
              "form": "one encryption per call (batch 1), device-resident, same kernels"}
+    # per-kernel device time of the plain form, from a few more calls profiled apart from the
+    # timed ones (the per-launch events would add to the measured latency)
+    ctx.profile_reset()
+    ctx.profile(True)
+    npr = 4
+    for i in range(npr):
+        ctx.encrypt(x_dev[i:i + 1], mpk, seeds2[i:i + 1], seeds3[i:i + 1], ct=pl_ct)
+        ctx.decrypt(pl_ct, y_dev, sky, y_signed=True, dy=pl_dy)
+        ctx.decode(pl_dy, out=pl_out)
+        torch.cuda.synchronize()
+    ctx.profile(False)
+    plain_prof = ctx.profile_read()
 
     # --- batched with the constant-coefficient decrypt (decrypt + decode of coefficient 0 only)
     r0 = torch.empty((steps, B, 1), dtype=torch.int32, device=dev)
@@ -436,17 +448,27 @@ def gpu_arm(args):
             "algorithmic_bytes": abytes,
             "share": tot / sum(v[1] for v in prof.values())}
     roof["frac"] = roof["achieved"] / hbm_peak if roof["achieved"] else None
-    if name.startswith("sample_cand"):
-        # the AES keystream bounds this kernel: 14 AES-256 blocks per refill; with the
-        # counter caching a block takes 1 + 4 + 11 x 16 + 16 = 197 T-table lookups from
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+
+    def lds_pipe(batch, launch_s):
+        # the AES keystream bounds the sigma_3 candidate kernel: 14 AES-256 blocks per refill;
+        # with the counter caching a block takes 1 + 4 + 11 x 16 + 16 = 197 T-table lookups from
         # shared memory, plus 15 per refill for the round-2 constants (one warp LDS per clock
         # per SM): 198 per block
-        blocks = refills3 * B * 14
-        sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        blocks = refills3 * batch * 14
         lds_peak = 148 * sm_mhz * 1e6 * 32 / 198
-        roof["pipe"] = {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)",
-                        "achieved": blocks / per_launch_s, "peak_lds_bound": lds_peak,
-                        "frac": blocks / per_launch_s / lds_peak, "sm_mhz": sm_mhz}
+        return {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)", "achieved": blocks / launch_s,
+                "peak_lds_bound": lds_peak, "frac": blocks / launch_s / lds_peak, "sm_mhz": sm_mhz}
+
+    if name.startswith("sample_cand"):
+        roof["pipe"] = lds_pipe(B, per_launch_s)
+    # the plain form: its dominant kernel, that kernel's share of the call, and its pipe fraction
+    pname, (pcnt, ptot) = max(plain_prof.items(), key=lambda kv: kv[1][1])
+    plain["roofline"] = {"kernel": pname, "ms_per_call": ptot / npr,
+                         "share_of_call_p50": ptot / npr / plain["p50_ms"],
+                         "device_ms_per_call": sum(v[1] for v in plain_prof.values()) / npr}
+    if pname == "sample_cand_s3":
+        plain["roofline"]["pipe"] = lds_pipe(1, ptot / pcnt / 1000.0)
 
     line = {"metric": METRIC, "value": ips, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warm,
             "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
