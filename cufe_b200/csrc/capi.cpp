@@ -316,7 +316,7 @@ int cufe_deserialize(cufe_ctx *h, int kind, int count, const uint8_t *d_src, siz
 }
 
 int cufe_sampler_call_search(int mode) {
-  if (mode < 0 || mode > 1) return CUFE_ERR_INVALID;
+  if (mode < 0 || mode > 2) return CUFE_ERR_INVALID;
   cufe::set_call_search(mode);
   return CUFE_OK;
 }

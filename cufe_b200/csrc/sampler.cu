@@ -872,12 +872,14 @@ static int doubling_levels(uint32_t max_calls) {
   while (k < 31 && (1u << k) <= max_calls) ++k;
   return k;  // bit_length(max_calls), at least 1
 }
-// Doubling costs about 3.2 ps per refill per table level (memory-bound gathers); the walk
-// about 0.7 us per call of its longest stream (serial dependent loads), both measured on a
-// B200.  Doubling is chosen when it is the cheaper of the two and its tables stay below 32 Mi
-// refills.
+// Doubling costs about 6.4 ps per refill per table level (memory-bound gathers); the walk
+// about 1.0-1.4 us per call of its longest stream (serial dependent loads), both measured on
+// a B200 (sigma_3 at n = 4096, l = 784: doubling 0.48 / 1.12 ms at 8 / 16 encryptions, walk
+// 0.78 ms up to 16 and 1.13 ms from 24).  Doubling is chosen when it is the cheaper of the two
+// and its tables stay below 32 Mi refills.
 bool seg_auto_doubling(uint64_t refills, uint32_t max_calls) {
   if (g_call_search == 1 || refills > kDoublingMaxRefills) return false;
+  if (g_call_search == 2) return true;
   return refills * (uint64_t)doubling_levels(max_calls) <= (uint64_t)max_calls * 200000u;
 }
 

@@ -161,9 +161,11 @@ int cufe_sample_gpu_map(cufe_ctx *ctx, int sig, const uint8_t key[32], int poly0
 int cufe_sample_polya(cufe_ctx *ctx, const uint8_t seed[32], uint32_t *d_a, void *stream);
 
 /* How the CPU-mapping samplers find where each gaussian_sampler_S* call starts (process-wide;
- * both give the same samples): 0 (default) pointer doubling for runs up to 32 Mi refills,
- * the serial walk above; 1 always the serial walk.  Applies to workspaces sized after the
- * call. */
+ * all give the same samples): 0 (default) the cheaper of pointer doubling (parallel over
+ * refills, log2(calls) table levels; runs up to 32 Mi refills) and the serial one-warp walk
+ * (dependent loads per call of the longest stream), by a cost model measured on a B200;
+ * 1 always the walk; 2 doubling whenever the run is within 32 Mi refills.  Applies to
+ * workspaces sized after the call. */
 int cufe_sampler_call_search(int mode);
 
 /* Serialized keys and ciphertexts: a 32-byte header (magic "CUFE", version 1, kind, n, l,

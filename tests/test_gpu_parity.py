@@ -102,23 +102,24 @@ def test_sampler_cpu_map(sig, rng, oracle_built):
 
 @pytest.mark.parametrize("sig", [0, 1, 2])
 def test_call_search_walk_equals_doubling(sig, rng, oracle_built):
-    """the two call-start searches give the same samples (uniform streams, and uneven ones
-    through a heterogeneous batch)"""
+    """the call-start searches (cost rule, walk, doubling) give the same samples (uniform
+    streams, and uneven ones through a heterogeneous batch)"""
     L = cf.lib()
+    assert L.cufe_sampler_call_search(3) != 0  # modes are 0, 1, 2
     c = cf.Context(1024, 8)
     keys = seeds(rng, 5)
     outs = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         assert L.cufe_sampler_call_search(mode) == 0
         outs.append(cf.u32(c.sample_cpu_map(sig, keys, 37)))
         c.sync()
     assert L.cufe_sampler_call_search(0) == 0
-    assert (outs[0] == outs[1]).all()
+    assert (outs[0] == outs[1]).all() and (outs[0] == outs[2]).all()
     c.close()
     if sig == 2:
         ns, ls = [256, 1024, 512], [5, 33, 12]
         res = []
-        for mode in (0, 1):
+        for mode in (1, 2):
             L.cufe_sampler_call_search(mode)
             B = cf.Batch(ns, ls)
             r = np.random.default_rng(9)
