@@ -258,6 +258,43 @@ def test_decrypt_coef0(n, l, rng, oracle_built):
     c.close()
 
 
+@pytest.mark.parametrize("n,l,B,K", [(256, 8, 70, 33), (2048, 124, 5, 129), (4096, 40, 65, 64)])
+def test_decrypt_coef0_tiled(n, l, B, K, rng, oracle_built):
+    """from 32 keys the constant-coefficient decrypt runs as a tiled product over K = l + n;
+    its residues and decoded values must equal the one-CTA-per-pair kernel's (keys passed
+    one at a time), for ragged tiles and for uint32 and signed y"""
+    c = cf.Context(n, l)
+    sa, se = seeds(rng, 2)
+    mpk, msk = c.setup(sa, None, se)
+    x = rng.integers(0, 5, (B, l), dtype=np.uint32)
+    ct = c.encrypt(dev(x), mpk, seeds(rng, B), None)
+    p = 64 * l + 1
+    for signed in (False, True):
+        if signed:
+            yi = rng.integers(-16, 17, (K, l), dtype=np.int64)
+            y = yi.astype(np.int32).view(np.uint32)
+        else:
+            y = rng.integers(0, 17, (K, l), dtype=np.uint32)
+            yi = y.astype(np.int64)
+        yd = dev(y)
+        sky = c.keygen(yd, msk, y_signed=signed)
+        d0 = dev(np.zeros((B, K, 3), np.uint32))
+        got = cf.u32(c.decrypt_coef0(ct, yd, sky, y_signed=signed, d0=d0))
+        got_nod0 = cf.u32(c.decrypt_coef0(ct, yd, sky, y_signed=signed))  # workspace for the residues
+        c.sync()
+        d0h = cf.u32(d0)
+        for k in range(K):
+            r0 = dev(np.zeros((B, 1, 3), np.uint32))
+            one = cf.u32(c.decrypt_coef0(ct, yd[k:k + 1], sky[k:k + 1], y_signed=signed, d0=r0))
+            c.sync()
+            assert (d0h[:, k] == cf.u32(r0)[:, 0]).all(), (signed, k)
+            assert (got[:, k] == one[:, 0]).all(), (signed, k)
+        assert (got_nod0 == got).all()
+        ip = (x.astype(np.int64) @ yi.T) % p
+        assert (got.astype(np.int64) % p == ip).all()
+    c.close()
+
+
 def test_scheme_gpu_map(rng, oracle_built):
     n, l = 1024, 16
     c = cf.Context(n, l)
