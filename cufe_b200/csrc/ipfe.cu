@@ -453,10 +453,12 @@ __global__ void __launch_bounds__(512) k_setup_mpk(const uint32_t *__restrict__ 
 }
 
 // Fused encryption (src/rlwe_sife.c:157-176): for instance b and residue polynomial
-// r = 3i + m of the ciphertext, c = INTT(pk_r * r^) + f + floor(q/p) x_i.  CTAs are ordered
-// residue-major so the instances of one pk polynomial run together (pk read once per batch).
-template <int LOGN>
-__global__ void __launch_bounds__(512)
+// r = 3i + m of the ciphertext, c = INTT(pk_r * r^) + f + floor(q/p) x_i.  A thread group
+// transforms PP instances (b, b + 1, ...) of one residue: one pk load, shared twiddles and
+// exchange addresses.  Work items are residue-major so the instances of one pk polynomial run
+// together (pk read once per batch).
+template <int LOGN, int PP, int MINB>
+__global__ void __launch_bounds__(NttPlan<LOGN>::T * ppc<LOGN>(), MINB)
     k_encrypt(const uint32_t *__restrict__ mpk, const uint32_t *__restrict__ rhat, const uint32_t *__restrict__ rhat_sh,
               long long rhat_stride, const uint32_t *__restrict__ f3, long long f3_stride,
               const uint32_t *__restrict__ f0, long long f0_stride, const uint32_t *__restrict__ x,
@@ -464,38 +466,51 @@ __global__ void __launch_bounds__(512)
   using P = NttPlan<LOGN>;
   extern __shared__ uint32_t smem_u32[];
   const int th = threadIdx.x;
+  const int bgroups = (batch + PP - 1) / PP;
   const long long wi = (long long)blockIdx.x * blockDim.y + threadIdx.y;
   const bool act = wi < nwork;
   const long long ww = act ? wi : nwork - 1;
   const int l = sa.l;
-  const long long res = ww / batch;
-  const int b = (int)(ww - res * batch);
+  const long long res = ww / bgroups;
+  const int b0 = (int)(ww - res * bgroups) * PP;
   const int m = (int)(res % 3), i = (int)(res / 3);
   const uint32_t q = sa.ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
-  uint32_t a[16], w[16], wsh[16];
-  load16(mpk + res * P::N + th * 16, a);
-  load16(rhat + b * rhat_stride + (size_t)m * P::N + th * 16, w);
-  load16(rhat_sh + b * rhat_stride + (size_t)m * P::N + th * 16, wsh);
+  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::N;
+  uint32_t a[PP][16];
+  {
+    uint32_t pk[16];
+    load16(mpk + res * P::N + th * 16, pk);
 #pragma unroll
-  for (int e = 0; e < 16; ++e) a[e] = shoup_mul(a[e], w[e], wsh[e], q);
-  ntt_inv_core<LOGN>(a, sm, th, q, sa.ra.ipsi2 + (size_t)m * P::N, sa.ra.ninv[m],
-                     sa.ra.ninv_sh[m], sa.ra.w1n[m], sa.ra.w1n_sh[m]);
-  const uint32_t *f;
-  uint32_t msg = 0;
-  if (i < l) {
-    f = f3 + b * f3_stride + ((size_t)i * 3 + m) * P::N;
-    const uint32_t xr = mod_u64(x[(size_t)b * l + i], sa.mu[m], q);
-    msg = shoup_mul(xr, sa.delta_mod[m], sa.delta_sh[m], q);
-  } else {
-    f = f0 + b * f0_stride + (size_t)m * P::N;
+    for (int p = 0; p < PP; ++p) {
+      const int b = min(b0 + p, batch - 1);  // a dead slot repeats the last instance, stores nothing
+      uint32_t w[16], wsh[16];
+      load16(rhat + b * rhat_stride + (size_t)m * P::N + th * 16, w);
+      load16(rhat_sh + b * rhat_stride + (size_t)m * P::N + th * 16, wsh);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) a[p][e] = shoup_mul(pk[e], w[e], wsh[e], q);
+    }
   }
-  uint32_t *c = ct + ((size_t)b * (l + 1) * 3 + res) * P::N;
-  if (act) {
+  ntt_inv_core<LOGN, PP>(a, sm, th, q, sa.ra.ipsi2 + (size_t)m * P::N, sa.ra.ninv[m], sa.ra.ninv_sh[m],
+                         sa.ra.w1n[m], sa.ra.w1n_sh[m]);
+  if (!act) return;
+#pragma unroll
+  for (int p = 0; p < PP; ++p) {
+    const int b = b0 + p;
+    if (b >= batch) break;
+    const uint32_t *f;
+    uint32_t msg = 0;
+    if (i < l) {
+      f = f3 + b * f3_stride + ((size_t)i * 3 + m) * P::N;
+      const uint32_t xr = mod_u64(x[(size_t)b * l + i], sa.mu[m], q);
+      msg = shoup_mul(xr, sa.delta_mod[m], sa.delta_sh[m], q);
+    } else {
+      f = f0 + b * f0_stride + (size_t)m * P::N;
+    }
+    uint32_t *c = ct + ((size_t)b * (l + 1) * 3 + res) * P::N;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
       const int j = P::template idx<0>(th, e);
-      c[j] = mod_add(mod_add(a[e], f[j], q), msg, q);
+      c[j] = mod_add(mod_add(a[p][e], f[j], q), msg, q);
     }
   }
 }
@@ -1007,11 +1022,21 @@ static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *
   const SchemeArgs sa = scheme_args(c);
   return dispatch_logn(c.ring.logn, [&](auto L) {
     constexpr int LOGN = decltype(L)::value;
-    constexpr int G = ppc<LOGN>();
-    CUFE_CUDA(cudaFuncSetAttribute(k_encrypt<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    constexpr int G = ppc<LOGN>(), NT = NttPlan<LOGN>::T * G;
+    constexpr int MINB = NT >= 1024 ? 1 : 1024 / NT;  // 64 registers
     ProfScope ps("encrypt_intt", s);
-    k_encrypt<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
-        d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
+    if (batch >= 2) {  // two instances per thread group
+      auto kern = k_encrypt<LOGN, 2, MINB>;
+      const long long nw = (long long)(c.l + 1) * 3 * ((batch + 1) / 2);
+      CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+      kern<<<(unsigned)((nw + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * 2 * NttPlan<LOGN>::N * 4, s>>>(
+          d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nw, sa);
+    } else {
+      auto kern = k_encrypt<LOGN, 1, MINB>;
+      CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+      kern<<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+          d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
+    }
     CUFE_CUDA(cudaGetLastError());
     return CUFE_OK;
   });
