@@ -339,6 +339,7 @@ def gpu_arm(args):
     clocks = clk.stop()
     ctx.profile(False)
     prof = ctx.profile_read()
+    timed_launches = ctx.profile_launches()
     ctx.sync()
     step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(steps)]
     ms = max_over_ranks(ms, dev)
@@ -430,7 +431,7 @@ def gpu_arm(args):
     # --- roofline of the dominant kernel (device time summed over the timed region)
     from cufe_b200 import _refills_s3
     refills3 = _refills_s3(N, L)
-    launches = sum(v[0] for v in prof.values())
+    launches = timed_launches
     dom = max(prof.items(), key=lambda kv: kv[1][1])
     name, (cnt, tot) = dom
     per_launch_s = tot / cnt / 1000.0
@@ -946,6 +947,7 @@ def svm_workload(args):
     clocks = clk.stop()
     c.profile(False)
     prof = c.profile_read()
+    svm_launches = c.profile_launches()
     ms = e0.elapsed_time(e1)
     p = 64 * l + 1
     ip = x.astype(np.int64) @ sv.astype(np.int64).T
@@ -961,7 +963,7 @@ def svm_workload(args):
             "data": "synthetic", "bit_exact": ok, "sv_keys_s": keys_s,
             "config": {"workload": "1,000 test vectors (a1a-shaped) x 500 support vectors, encrypt + predict per step",
                        "n": n, "l": l, "test_vectors": ntest, "support_vectors": nsv},
-            "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+            "gpu_launches": svm_launches, "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "clocks": clocks}
     if not args.no_cpu_baseline:
         import multiprocessing as mp

@@ -55,6 +55,7 @@ def lib():
             "cufe_profile_enable": [vp, i],
             "cufe_profile_read": [vp, i, vp, vp, vp],
             "cufe_profile_reset": [vp],
+            "cufe_profile_launches": [vp],
             "cufe_tables": [vp, vp, vp],
             "cufe_setup": [vp, vp, vp, vp, vp, vp, vp],
             "cufe_setup_gpu_map": [vp, vp, vp, vp, vp, vp],
@@ -118,6 +119,7 @@ def lib():
             f.restype = None if name.startswith("rlwe_sife_") else C.c_int
         L.cufe_sampler_refills.restype = C.c_longlong
         L.cufe_serialized_bytes.restype = C.c_longlong
+        L.cufe_profile_launches.restype = C.c_longlong
         for name in ("cufe_server_encrypt", "cufe_server_keygen", "cufe_server_decrypt"):
             getattr(L, name).restype = C.c_longlong
         L.cufe_server_now.argtypes = []
@@ -223,8 +225,15 @@ class Context:
     def profile_reset(self):
         _check(lib().cufe_profile_reset(self.h), "cufe_profile_reset")
 
+    def profile_launches(self):
+        """kernel launches of this context while profiling was on, since the last reset"""
+        n = lib().cufe_profile_launches(self.h)
+        if n < 0:
+            raise CufeError(int(n), "cufe_profile_launches")
+        return int(n)
+
     def profile_read(self):
-        """{kernel name: (launches, total ms)} since the last reset"""
+        """{group name: (kernel launches, total ms)} since the last reset"""
         names = C.create_string_buffer(64 * 64)
         launches = np.zeros(64, np.int64)
         ms = np.zeros(64, np.float64)

@@ -487,7 +487,7 @@ int Batch::run(cudaStream_t s) {
       attr = true;
     }
     ProfScope ps("batch_keygen", s);
-    k_keygen_het<<<keygen_units, 256, smem, s>>>(reinterpret_cast<const InstDev *>(tables + keygen_inst_off),
+    note_launch(), k_keygen_het<<<keygen_units, 256, smem, s>>>(reinterpret_cast<const InstDev *>(tables + keygen_inst_off),
                                                  reinterpret_cast<const uint64_t *>(tables + keygen_unit_off),
                                                  (uint32_t)count, keys, y, sky, mq);
     CUFE_CUDA(cudaGetLastError());
@@ -524,7 +524,7 @@ int Batch::run(cudaStream_t s) {
           attr = true;
         }
         ProfScope ps("batch_encrypt", s);
-        k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, s>>>(
+        note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, s>>>(
             reinterpret_cast<const InstDev *>(tables + g.inst_off), reinterpret_cast<const uint64_t *>(tables + g.res_off),
             g.count, g.nres, keys, rh, rhsh, f3, s2o, x, ct, ra, mq);
         CUFE_CUDA(cudaGetLastError());
@@ -534,7 +534,7 @@ int Batch::run(cudaStream_t s) {
     }
     {
       ProfScope ps("batch_decrypt", s);
-      k_dec_coef0_het<<<ch.count, 256, 0, s>>>(reinterpret_cast<const InstDev *>(tables + ch.inst_off), ct, sky, y,
+      note_launch(), k_dec_coef0_het<<<ch.count, 256, 0, s>>>(reinterpret_cast<const InstDev *>(tables + ch.inst_off), ct, sky, y,
                                               out, d0, mq, dd);
       CUFE_CUDA(cudaGetLastError());
     }
@@ -1001,7 +1001,7 @@ struct Server {
             attr = true;
           }
           ProfScope ps("serve_encrypt", stream);
-          k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, stream>>>(
+          note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, stream>>>(
               reinterpret_cast<const InstDev *>(d_tab + g.inst_off), reinterpret_cast<const uint64_t *>(d_tab + g.res_off),
               g.count, g.nres, tenants.keys, rh, rhsh, f3, s2o, xd, d_ct, ra, tenants.mq);
           CUFE_CUDA(cudaGetLastError());
@@ -1017,14 +1017,14 @@ struct Server {
         attr = true;
       }
       ProfScope ps("serve_keygen", stream);
-      k_keygen_het<<<(unsigned)uo.back(), 256, (size_t)2 * max_l * 4, stream>>>(
+      note_launch(), k_keygen_het<<<(unsigned)uo.back(), 256, (size_t)2 * max_l * 4, stream>>>(
           reinterpret_cast<const InstDev *>(d_tab + kg_inst), reinterpret_cast<const uint64_t *>(d_tab + kg_units),
           (uint32_t)kg.size(), tenants.keys, reinterpret_cast<const int32_t *>(d_sk), d_sk, tenants.mq);
       CUFE_CUDA(cudaGetLastError());
     }
     if (!dec.empty()) {
       ProfScope ps("serve_decrypt", stream);
-      k_dec_coef0_het<<<(unsigned)dec.size(), 256, 0, stream>>>(reinterpret_cast<const InstDev *>(d_tab + dec_inst),
+      note_launch(), k_dec_coef0_het<<<(unsigned)dec.size(), 256, 0, stream>>>(reinterpret_cast<const InstDev *>(d_tab + dec_inst),
                                                                d_ct, d_sk, reinterpret_cast<const int32_t *>(d_sk),
                                                                d_out, nullptr, tenants.mq, tenants.dd);
       CUFE_CUDA(cudaGetLastError());

@@ -12,6 +12,7 @@
 
 namespace cufe {
 thread_local Prof *t_prof = nullptr;
+thread_local long long t_launches = 0;
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 }  // namespace cufe
@@ -127,7 +128,13 @@ int cufe_profile_reset(cufe_ctx *h) {
   std::lock_guard<std::mutex> lk(h->c.mu);
   h->c.prof.collect();
   h->c.prof.acc.clear();
+  h->c.prof.kernels = 0;
   return CUFE_OK;
+}
+
+long long cufe_profile_launches(const cufe_ctx *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  return h->c.prof.kernels;
 }
 
 long long cufe_sampler_refills(int sig, int calls, int n) {

@@ -260,7 +260,7 @@ int launch_ntt_sel(const RingArgs &ra, const ModSel &sel, uint32_t *data, uint32
   const long long groups = (rows + PP - 1) / PP * sel.nm;
   const long long grid = (groups + G - 1) / G;
   if (grid <= 0) return CUFE_OK;
-  k_ntt<LOGN, MODE, PP, LBT, MINB, LE, SQ><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra, sel);
+  note_launch(), k_ntt<LOGN, MODE, PP, LBT, MINB, LE, SQ><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, rows, ra, sel);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -374,7 +374,7 @@ int launch_ntt_stream(const RingArgs &ra, uint32_t *data, uint32_t *sh, long lon
   const long long grid = std::min(need, (long long)device_sms() * occ);
   if (grid <= 0) return CUFE_OK;
   ProfScope ps(MODE == 2 ? "ntt_inverse" : "ntt_forward", s);
-  k_ntt_stream<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
+  note_launch(), k_ntt_stream<LOGN, MODE><<<(unsigned)grid, dim3(P::T, G), smem, s>>>(data, sh, nres, ra);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -956,7 +956,7 @@ static int setup_tail(Ctx &c, int l, uint32_t *d_mpk, const uint32_t *d_msk, uin
     constexpr int G = ppc<LOGN>();
     CUFE_CUDA(cudaFuncSetAttribute(k_setup_mpk<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     ProfScope ps("setup_mpk", s);
-    k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+    note_launch(), k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
         d_msk, e, ahat, a_sh, d_mpk, nres, c.ring.args);
     CUFE_CUDA(cudaGetLastError());
     return CUFE_OK;
@@ -1029,12 +1029,12 @@ static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *
       auto kern = k_encrypt<LOGN, 2, MINB>;
       const long long nw = (long long)(c.l + 1) * 3 * ((batch + 1) / 2);
       CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-      kern<<<(unsigned)((nw + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * 2 * NttPlan<LOGN>::N * 4, s>>>(
+      note_launch(), kern<<<(unsigned)((nw + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * 2 * NttPlan<LOGN>::N * 4, s>>>(
           d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nw, sa);
     } else {
       auto kern = k_encrypt<LOGN, 1, MINB>;
       CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-      kern<<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+      note_launch(), kern<<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
           d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
     }
     CUFE_CUDA(cudaGetLastError());
@@ -1116,7 +1116,7 @@ int ctx_keygen(Ctx &c, int nkeys, const uint32_t *d_y, int y_signed, const uint3
   CUFE_CUDA(cudaFuncSetAttribute(k_keygen<KCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((c.n + 255) / 256, 3, (nkeys + KCH - 1) / KCH);
   ProfScope ps("keygen", s);
-  k_keygen<KCH><<<grid, 256, smem, s>>>(d_y, y_signed, nkeys, d_msk, d_sky, c.n, sa);
+  note_launch(), k_keygen<KCH><<<grid, 256, smem, s>>>(d_y, y_signed, nkeys, d_msk, d_sky, c.n, sa);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -1154,7 +1154,7 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
     if (smem > 200 * 1024) return CUFE_ERR_INVALID;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_mac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ProfScope ps("decrypt_mac", s);
-    k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
+    note_launch(), k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
                                                                              part, sa);
     CUFE_CUDA(cudaGetLastError());
   }
@@ -1164,7 +1164,7 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
     const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     ProfScope ps("decrypt_tail", s);
-    k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
+    note_launch(), k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
         part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);
     CUFE_CUDA(cudaGetLastError());
     return (int)CUFE_OK;
@@ -1249,7 +1249,7 @@ int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t 
     const size_t smem = (size_t)2 * ((l + nsplit - 1) / nsplit + 1) * 4;
     if (smem > 200 * 1024) return CUFE_ERR_INVALID;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_mac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
+    note_launch(), k_dec_mac<<<dim3(per_poly * nsplit, (unsigned)nwork), threads, smem, s>>>(d_ct, d_y, y_signed, nkeys, nsplit,
                                                                              part, sa);
     CUFE_CUDA(cudaGetLastError());
   }
@@ -1258,7 +1258,7 @@ int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t 
     constexpr int G = ppc<LOGN>();
     const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-    k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
+    note_launch(), k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
         part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);
     CUFE_CUDA(cudaGetLastError());
     return (int)CUFE_OK;
@@ -1290,7 +1290,7 @@ int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_
   const DecodeArgs d = decode_args(c);
   const long long total = (long long)count * ncoeff;
   ProfScope ps("decode", s);
-  k_decode<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_dy, count, ncoeff, d_out, d);
+  note_launch(), k_decode<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_dy, count, ncoeff, d_out, d);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -1300,7 +1300,7 @@ int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const ui
   if (nct < 1 || nkeys < 1 || (long long)nct * nkeys > 0x7fffffffLL || !d_out) return CUFE_ERR_INVALID;
   if (nkeys < kCoef0TiledMinKeys || c.l + c.n >= (1 << 17)) {
     ProfScope ps("decrypt_coef0", s);
-    k_dec_coef0<<<(unsigned)(nct * nkeys), 256, 0, s>>>(d_ct, d_y, y_signed, nkeys, d_sky, d_d0, d_out,
+    note_launch(), k_dec_coef0<<<(unsigned)(nct * nkeys), 256, 0, s>>>(d_ct, d_y, y_signed, nkeys, d_sky, d_d0, d_out,
                                                         scheme_args(c), decode_args(c));
     CUFE_CUDA(cudaGetLastError());
     return CUFE_OK;
@@ -1315,9 +1315,9 @@ int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const ui
   }
   ProfScope ps("decrypt_coef0", s);
   const dim3 grid((unsigned)((nct + kC0Tile - 1) / kC0Tile), (unsigned)((nkeys + kC0Tile - 1) / kC0Tile), 3);
-  k_dec_coef0_tiled<<<grid, 256, 0, s>>>(d_ct, d_y, y_signed, nct, nkeys, d_sky, d0, scheme_args(c));
+  note_launch(), k_dec_coef0_tiled<<<grid, 256, 0, s>>>(d_ct, d_y, y_signed, nct, nkeys, d_sky, d0, scheme_args(c));
   CUFE_CUDA(cudaGetLastError());
-  k_decode_triples<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(d0, npairs, d_out, decode_args(c));
+  note_launch(), k_decode_triples<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(d0, npairs, d_out, decode_args(c));
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }

@@ -761,7 +761,7 @@ __global__ void k_expand_keys(const uint8_t *__restrict__ seeds, const uint32_t 
 int expand_keys_device(const uint8_t *d_seeds, const uint32_t *d_perm, uint32_t count, uint32_t *d_rk,
                        cudaStream_t s) {
   if (!count) return CUFE_OK;
-  k_expand_keys<<<(count + 127) / 128, 128, 0, s>>>(d_seeds, d_perm, count, d_rk);
+  note_launch(), k_expand_keys<<<(count + 127) / 128, 128, 0, s>>>(d_seeds, d_perm, count, d_rk);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -916,17 +916,17 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
   if (grid > 0) {
     ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
     if (sig == 0)
-      k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
     else if (sig == 1)
-      k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
     else
-      k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
   }
   CUFE_CUDA(cudaGetLastError());
   if (z.tiles) {
     ProfScope ps("sample_scan", s);
-    k_scan_tiles<<<z.tiles, 512, 0, s>>>(amask, sg, elocal, tsum);
-    k_scan_sums<<<z.nstreams, 1024, 0, s>>>(tsum, sg);
+    note_launch(), k_scan_tiles<<<z.tiles, 512, 0, s>>>(amask, sg, elocal, tsum);
+    note_launch(), k_scan_sums<<<z.nstreams, 1024, 0, s>>>(tsum, sg);
   }
   if (z.doubling) {
     const int levels = doubling_levels(z.max_calls);
@@ -934,18 +934,18 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
     const uint64_t stride = align256(z.refills * 4) / 4;
     ProfScope ps("sample_walk", s);
     const unsigned rg = (unsigned)((z.refills + 255) / 256);
-    k_next_start<<<rg, 256, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), tab);
-    for (int k = 1; k < levels; ++k) k_next_square<<<rg, 256, 0, s>>>(tab + (k - 1) * stride, tab + k * stride, sg);
-    k_starts_from_tables<<<(unsigned)((z.calls + z.nstreams + 255) / 256), 256, 0, s>>>(tab, levels, stride, sg,
+    note_launch(), k_next_start<<<rg, 256, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), tab);
+    for (int k = 1; k < levels; ++k) note_launch(), k_next_square<<<rg, 256, 0, s>>>(tab + (k - 1) * stride, tab + k * stride, sg);
+    note_launch(), k_starts_from_tables<<<(unsigned)((z.calls + z.nstreams + 255) / 256), 256, 0, s>>>(tab, levels, stride, sg,
                                                                                         cstart, d_status);
   } else {
     ProfScope ps("sample_walk", s);
-    k_walk<<<(z.nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), cstart, d_status);
+    note_launch(), k_walk<<<(z.nstreams + 3) / 4, 128, 0, s>>>(elocal, tsum, amask, sg, (float)mean_accept(sig), cstart, d_status);
   }
   CUFE_CUDA(cudaGetLastError());
   if (d_out && z.calls) {
     ProfScope ps_sc("sample_scatter", s);
-    k_scatter<<<(uint32_t)z.calls, kScatterThreads, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
+    note_launch(), k_scatter<<<(uint32_t)z.calls, kScatterThreads, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
     CUFE_CUDA(cudaGetLastError());
   }
   return CUFE_OK;
@@ -960,7 +960,7 @@ static int seg_uniform(uint32_t nstreams, uint32_t calls, uint32_t n, int sig, v
   uint8_t *b = static_cast<uint8_t *>(ws);
   *sg = seg_bind(b, nstreams);
   const uint32_t R = (uint32_t)(z->refills / nstreams);
-  k_seg_uniform<<<(nstreams + 256) / 256, 256, 0, s>>>(
+  note_launch(), k_seg_uniform<<<(nstreams + 256) / 256, 256, 0, s>>>(
       nstreams, calls, n, R, z->tiles / nstreams, (uint64_t)calls * 3 * n, reinterpret_cast<uint32_t *>(b + L.n),
       reinterpret_cast<uint32_t *>(b + L.calls), reinterpret_cast<uint64_t *>(b + L.roff),
       reinterpret_cast<uint32_t *>(b + L.toff), reinterpret_cast<uint64_t *>(b + L.coff),
@@ -987,11 +987,11 @@ int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npo
   const double kinv = kinv_of(sig);
   ProfScope ps("sample_gpu_map", s);
   if (sig == 0)
-    k_gauss_gpu_map<0><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<0><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
   else if (sig == 1)
-    k_gauss_gpu_map<1><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<1><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
   else
-    k_gauss_gpu_map<2><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<2><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
@@ -999,7 +999,7 @@ int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npo
 int sample_polya(const uint32_t *d_rkey, uint32_t n, uint32_t *d_a, cudaStream_t s) {
   const uint32_t grid = (n / 2 + 255) / 256;
   ProfScope ps("sample_polya", s);
-  k_polya<<<grid, 256, kAesSmemBytes, s>>>(d_rkey, n, mod_args(), d_a);
+  note_launch(), k_polya<<<grid, 256, kAesSmemBytes, s>>>(d_rkey, n, mod_args(), d_a);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }

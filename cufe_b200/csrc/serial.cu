@@ -136,7 +136,7 @@ int ctx_serialize(Ctx &c, int kind, int count, const uint32_t *d_src, uint8_t *d
   CUFE_CUDA(cudaMemsetAsync(d_dst + sizeof(h), 0, (size_t)h.payload, s));
   const uint64_t groups = (uint64_t)count * polys * ((c.n + 31) / 32);
   ProfScope ps("serialize", s);
-  k_pack<<<(unsigned)((groups + 255) / 256), 256, 0, s>>>(d_src, reinterpret_cast<uint32_t *>(d_dst + sizeof(h)),
+  note_launch(), k_pack<<<(unsigned)((groups + 255) / 256), 256, 0, s>>>(d_src, reinterpret_cast<uint32_t *>(d_dst + sizeof(h)),
                                                          (uint32_t)c.n, polys, groups, kRefPrimes[0], kRefPrimes[1],
                                                          kRefPrimes[2]);
   CUFE_CUDA(cudaGetLastError());
@@ -169,7 +169,7 @@ int ctx_deserialize(Ctx &c, int kind, int count, const uint8_t *d_src, size_t sr
   const uint64_t groups = (uint64_t)count * polys * ((c.n + 31) / 32);
   {
     ProfScope ps("deserialize", s);
-    k_unpack<<<(unsigned)((groups + 255) / 256), 256, 0, s>>>(reinterpret_cast<const uint32_t *>(d_src + sizeof(h)),
+    note_launch(), k_unpack<<<(unsigned)((groups + 255) / 256), 256, 0, s>>>(reinterpret_cast<const uint32_t *>(d_src + sizeof(h)),
                                                              d_dst, (uint32_t)c.n, polys, groups, kRefPrimes[0],
                                                              kRefPrimes[1], kRefPrimes[2], bad);
   }

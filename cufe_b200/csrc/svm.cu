@@ -144,7 +144,7 @@ int svm_predict(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *d_label
   int rc = ctx_decrypt_coef0(c, nct, d_ct, m.lsv, m.d_y, m.y_signed, m.d_sky, nullptr, kv, s);
   if (rc) return rc;
   ProfScope ps("svm_vote", s);
-  k_svm_vote<<<(nct + 127) / 128, 128, 0, s>>>(kv, nct, m.lsv, c.p, m.y_signed, m.nr_class, m.d_coef, m.d_rho,
+  note_launch(), k_svm_vote<<<(nct + 127) / 128, 128, 0, s>>>(kv, nct, m.lsv, c.p, m.y_signed, m.nr_class, m.d_coef, m.d_rho,
                                                m.d_nsv, m.d_label, d_label, d_dec);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;

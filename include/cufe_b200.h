@@ -84,13 +84,16 @@ int cufe_destroy(cufe_ctx *ctx);
 int cufe_sync(cufe_ctx *ctx, void *stream);
 /* a non-blocking stream owned by the context */
 void *cufe_ctx_stream(cufe_ctx *ctx);
-/* per-kernel device timing: when enabled, every kernel this context launches is bracketed
- * by CUDA events on its stream; cufe_profile_read waits for them and returns, per kernel
- * name (64-byte slots), the launch count and the summed milliseconds; returns the number
- * of kernels written (or a negative status) */
+/* per-kernel device timing: when enabled, every named group of launches (one kernel, or a
+ * few for a sampler stage) is bracketed by CUDA events on its stream; cufe_profile_read
+ * waits for them and returns, per group name (64-byte slots), the kernels launched in it and
+ * the summed milliseconds; returns the number of groups written (or a negative status) */
 int cufe_profile_enable(cufe_ctx *ctx, int on);
 int cufe_profile_read(cufe_ctx *ctx, int max_kernels, char *names, long long *launches, double *ms);
 int cufe_profile_reset(cufe_ctx *ctx);
+/* kernel launches of this context's calls while profiling was on, since the last reset (every
+ * kernel, inside a named group or not).  No counterpart in the reference. */
+long long cufe_profile_launches(const cufe_ctx *ctx);
 /* p and floor(q/p) mod q_j */
 int cufe_params(const cufe_ctx *ctx, uint32_t *p, uint32_t delta_mod[3]);
 /* twiddle tables [3][n] (psi^{bitrev(i)}, psi^{-bitrev(i)}) in host memory */
