@@ -683,39 +683,46 @@ __global__ void __launch_bounds__(256)
 // l + n: for modulus m = blockIdx.z,
 //   d0[c][key][m] = sum_{k<l} c_k[0] y_k + sum_{t<n} c_l[t] b_t,  b_0 = -s[0], b_t = s[n-t],
 // the negacyclic constant term of c_l * sk_y with its sign folded into the key operand.  A CTA
-// computes a 64 x 64 tile of (ciphertext, key) pairs, 4 x 4 per thread, from 32-deep K chunks
-// staged in shared memory (both operands reused 64 times).  Products are exact: A = a1 2^16 +
-// a0 with a0 < 2^16, a1 < 2^15, and two 64-bit sums s0 = sum a0 b, s1 = sum a1 b (one wide
-// multiply-add each; no overflow for K < 2^17), reduced once per pair.
-constexpr int kC0Tile = 64, kC0Kc = 32;
+// computes 64 ciphertexts x 32 keys, 4 x 2 per thread, from 32-deep K chunks staged in shared
+// memory (A reused 32 times, B 64 times).  Products are exact: a, b < 2^31, so four products
+// sum below 2^64 in one wide multiply-add chain, folded into a 64 + 32-bit accumulator (K < 2^34
+// products); one reduction per pair.
+constexpr int kC0Tm = 64, kC0Tn = 32, kC0Kc = 32;
 constexpr int kCoef0TiledMinKeys = 32;  // fewer keys: one CTA per pair
-__device__ __forceinline__ int c0_swz(int kk, int i) { return kk * kC0Tile + (i ^ ((kk & 15) << 2)); }
+__device__ __forceinline__ int c0_swz_a(int kk, int i) { return kk * kC0Tm + (i ^ ((kk & 15) << 2)); }
+__device__ __forceinline__ int c0_swz_b(int kk, int j) { return kk * kC0Tn + (j ^ ((kk & 15) << 1)); }
 
 __global__ void __launch_bounds__(256) k_dec_coef0_tiled(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ y,
                                                          int y_signed, int nct, int nkeys,
                                                          const uint32_t *__restrict__ sky, uint32_t *__restrict__ d0,
                                                          SchemeArgs sa) {
-  __shared__ __align__(16) uint32_t As[kC0Kc * kC0Tile], Bs[kC0Kc * kC0Tile];
+  __shared__ __align__(16) uint32_t As[kC0Kc * kC0Tm];
+  __shared__ __align__(16) uint32_t Bs[kC0Kc * kC0Tn];
   const int m = blockIdx.z, n = sa.ra.n, l = sa.l, K = l + n;
   const uint32_t q = sa.ra.q[m];
   const uint64_t mu = sa.mu[m];
-  const int ct0 = blockIdx.x * kC0Tile, key0 = blockIdx.y * kC0Tile;
+  const int ct0 = blockIdx.x * kC0Tm, key0 = blockIdx.y * kC0Tn;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  uint64_t s0[4][4], s1[4][4];
+  uint64_t lo[4][2];
+  uint32_t hi[4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) s0[i][j] = s1[i][j] = 0;
+    for (int j = 0; j < 2; ++j) lo[i][j] = 0, hi[i][j] = 0;
   for (int k0 = 0; k0 < K; k0 += kC0Kc) {
     // lane-consecutive k: the c_l and sk_y parts are contiguous runs per row
-    for (int e = threadIdx.x; e < kC0Tile * kC0Kc; e += blockDim.x) {
-      const int i = e / kC0Kc, kk = e % kC0Kc, k = k0 + kk;
-      uint32_t a = 0, b = 0;
-      const int c = ct0 + i, key = key0 + i;
+    for (int e = threadIdx.x; e < kC0Tm * kC0Kc; e += blockDim.x) {
+      const int i = e / kC0Kc, kk = e % kC0Kc, k = k0 + kk, c = ct0 + i;
+      uint32_t a = 0;
       if (k < K && c < nct) {
         const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * n;
         a = k < l ? cb[((size_t)k * 3 + m) * n] : cb[((size_t)l * 3 + m) * n + (k - l)];
       }
+      As[c0_swz_a(kk, i)] = a;
+    }
+    for (int e = threadIdx.x; e < kC0Tn * kC0Kc; e += blockDim.x) {
+      const int j = e / kC0Kc, kk = e % kC0Kc, k = k0 + kk, key = key0 + j;
+      uint32_t b = 0;
       if (k < K && key < nkeys) {
         if (k < l) {
           b = y_residue(y[(size_t)key * l + k], y_signed, q, mu);
@@ -725,37 +732,42 @@ __global__ void __launch_bounds__(256) k_dec_coef0_tiled(const uint32_t *__restr
           b = t == 0 ? (sk[0] ? q - sk[0] : 0u) : sk[n - t];
         }
       }
-      As[c0_swz(kk, i)] = a;
-      Bs[c0_swz(kk, i)] = b;
+      Bs[c0_swz_b(kk, j)] = b;
     }
     __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < kC0Kc; ++kk) {
-      const uint4 av = *reinterpret_cast<const uint4 *>(&As[c0_swz(kk, ty * 4)]);
-      const uint4 bv = *reinterpret_cast<const uint4 *>(&Bs[c0_swz(kk, tx * 4)]);
-      const uint32_t a[4] = {av.x, av.y, av.z, av.w}, b[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll 2
+    for (int kk = 0; kk < kC0Kc; kk += 4) {
+      uint32_t a[4][4], b[4][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const uint32_t a0 = a[i] & 0xffffu, a1 = a[i] >> 16;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          s0[i][j] += (uint64_t)a0 * b[j];
-          s1[i][j] += (uint64_t)a1 * b[j];
-        }
+      for (int u = 0; u < 4; ++u) {
+        const uint4 av = *reinterpret_cast<const uint4 *>(&As[c0_swz_a(kk + u, ty * 4)]);
+        const uint2 bv = *reinterpret_cast<const uint2 *>(&Bs[c0_swz_b(kk + u, tx * 2)]);
+        a[u][0] = av.x, a[u][1] = av.y, a[u][2] = av.z, a[u][3] = av.w;
+        b[u][0] = bv.x, b[u][1] = bv.y;
       }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          uint64_t t = (uint64_t)a[0][i] * b[0][j];
+#pragma unroll
+          for (int u = 1; u < 4; ++u) t += (uint64_t)a[u][i] * b[u][j];
+          const uint64_t nl = lo[i][j] + t;
+          hi[i][j] += nl < t;
+          lo[i][j] = nl;
+        }
     }
     __syncthreads();
   }
+  const uint64_t c64 = 0ull - mu * q;  // 2^64 mod q
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int c = ct0 + ty * 4 + i;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int key = key0 + tx * 4 + j;
-      if (c < nct && key < nkeys) {
-        const uint64_t hi = (uint64_t)mod_u64(s1[i][j], mu, q) << 16;
-        d0[((size_t)c * nkeys + key) * 3 + m] = mod_u64(hi + mod_u64(s0[i][j], mu, q), mu, q);
-      }
+    for (int j = 0; j < 2; ++j) {
+      const int key = key0 + tx * 2 + j;
+      if (c < nct && key < nkeys)
+        d0[((size_t)c * nkeys + key) * 3 + m] = mod_u64(mod_u64(lo[i][j], mu, q) + (uint64_t)hi[i][j] * c64, mu, q);
     }
   }
 }
@@ -1298,7 +1310,7 @@ int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_
 int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                       const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s) {
   if (nct < 1 || nkeys < 1 || (long long)nct * nkeys > 0x7fffffffLL || !d_out) return CUFE_ERR_INVALID;
-  if (nkeys < kCoef0TiledMinKeys || c.l + c.n >= (1 << 17)) {
+  if (nkeys < kCoef0TiledMinKeys) {
     ProfScope ps("decrypt_coef0", s);
     note_launch(), k_dec_coef0<<<(unsigned)(nct * nkeys), 256, 0, s>>>(d_ct, d_y, y_signed, nkeys, d_sky, d_d0, d_out,
                                                         scheme_args(c), decode_args(c));
@@ -1314,7 +1326,7 @@ int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const ui
     d0 = reinterpret_cast<uint32_t *>(c.ws);
   }
   ProfScope ps("decrypt_coef0", s);
-  const dim3 grid((unsigned)((nct + kC0Tile - 1) / kC0Tile), (unsigned)((nkeys + kC0Tile - 1) / kC0Tile), 3);
+  const dim3 grid((unsigned)((nct + kC0Tm - 1) / kC0Tm), (unsigned)((nkeys + kC0Tn - 1) / kC0Tn), 3);
   note_launch(), k_dec_coef0_tiled<<<grid, 256, 0, s>>>(d_ct, d_y, y_signed, nct, nkeys, d_sky, d0, scheme_args(c));
   CUFE_CUDA(cudaGetLastError());
   note_launch(), k_decode_triples<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(d0, npairs, d_out, decode_args(c));
