@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcufe_b200.so")
-SOURCES = ["ipfe.cu", "sampler.cu", "batch.cu", "svm.cu", "serial.cu", "capi.cpp"]
+SOURCES = ["ipfe.cu", "sampler.cu", "batch.cu", "svm.cu", "serial.cu", "staging.cpp", "capi.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr", "-Xptxas", "-O3"]

@@ -9,6 +9,7 @@
 
 #include "ctx.h"
 #include "sampler_host.h"
+#include "staging.h"
 
 namespace cufe {
 thread_local Prof *t_prof = nullptr;
@@ -388,6 +389,7 @@ struct Dropin {
   int status = CUFE_OK;
   uint32_t *buf = nullptr;
   size_t buf_words = 0;
+  cufe::Staging stage;  // the caller's pageable buffers <-> device, through pinned slots
 };
 Dropin &dropin() {
   static Dropin d;
@@ -492,8 +494,8 @@ void rlwe_sife_setup_gpu(uint32_t *mpk, uint32_t *msk, unsigned char *seed2, uns
   DI_CUDA(cudaMemcpy(dm + L * poly, mpk + L * poly, poly * 4, cudaMemcpyHostToDevice));
   DI_CHECK(cufe_setup_gpu_map(d.ctx, seed2, seed3, dm, ds, nullptr));
   DI_CHECK(cufe_sync(d.ctx, nullptr));
-  DI_CUDA(cudaMemcpy(mpk, dm, (L + 1) * poly * 4, cudaMemcpyDeviceToHost));
-  DI_CUDA(cudaMemcpy(msk, ds, L * poly * 4, cudaMemcpyDeviceToHost));
+  DI_CUDA(d.stage.d2h(mpk, dm, (L + 1) * poly * 4, nullptr));
+  DI_CUDA(d.stage.d2h(msk, ds, L * poly * 4, nullptr));
 }
 
 void rlwe_sife_encrypt_gpu(uint32_t *m, uint32_t *mpk, uint32_t *c, unsigned char *seed2, unsigned char *seed3,
@@ -513,11 +515,11 @@ void rlwe_sife_encrypt_gpu(uint32_t *m, uint32_t *mpk, uint32_t *c, unsigned cha
   Timer tm(part2_time);
   DI_CHECK(dropin_buf(d, (L + 1) * poly * (1 + R) + R * L));
   uint32_t *dm = d.buf, *dc = d.buf + (L + 1) * poly, *dx = dc + R * (L + 1) * poly;
-  DI_CUDA(cudaMemcpy(dm, mpk, (L + 1) * poly * 4, cudaMemcpyHostToDevice));
+  DI_CUDA(d.stage.h2d(dm, mpk, (L + 1) * poly * 4, nullptr));
   DI_CUDA(cudaMemcpy(dx, m, R * L * 4, cudaMemcpyHostToDevice));
   DI_CHECK(cufe_encrypt_gpu_map(d.ctx, repeat, dx, dm, seed2, dc, nullptr));
   DI_CHECK(cufe_sync(d.ctx, nullptr));
-  DI_CUDA(cudaMemcpy(c, dc, R * (L + 1) * poly * 4, cudaMemcpyDeviceToHost));
+  DI_CUDA(d.stage.d2h(c, dc, R * (L + 1) * poly * 4, nullptr));
 }
 
 void rlwe_sife_keygen_gpu(const uint32_t *y, const uint32_t *msk, uint32_t *sk_y, int repeat, float *part2_time) {
@@ -535,11 +537,11 @@ void rlwe_sife_keygen_gpu(const uint32_t *y, const uint32_t *msk, uint32_t *sk_y
   Timer tm(part2_time);
   DI_CHECK(dropin_buf(d, L * poly + R * poly + R * L));
   uint32_t *ds = d.buf, *dk = ds + L * poly, *dy = dk + R * poly;
-  DI_CUDA(cudaMemcpy(ds, msk, L * poly * 4, cudaMemcpyHostToDevice));
+  DI_CUDA(d.stage.h2d(ds, msk, L * poly * 4, nullptr));
   DI_CUDA(cudaMemcpy(dy, y, R * L * 4, cudaMemcpyHostToDevice));
   DI_CHECK(cufe_keygen(d.ctx, repeat, dy, 0, ds, dk, nullptr));
   DI_CHECK(cufe_sync(d.ctx, nullptr));
-  DI_CUDA(cudaMemcpy(sk_y, dk, R * poly * 4, cudaMemcpyDeviceToHost));
+  DI_CUDA(d.stage.d2h(sk_y, dk, R * poly * 4, nullptr));
 }
 
 void rlwe_sife_decrypt_gmp_gpu(uint32_t *c, const uint32_t *y, uint32_t *sk_y, uint32_t *d_y, int repeat,
@@ -558,12 +560,12 @@ void rlwe_sife_decrypt_gmp_gpu(uint32_t *c, const uint32_t *y, uint32_t *sk_y, u
   Timer tm(part2_time);
   DI_CHECK(dropin_buf(d, (L + 1) * poly + 2 * R * poly + R * L));
   uint32_t *dc = d.buf, *dk = dc + (L + 1) * poly, *dd = dk + R * poly, *dy = dd + R * poly;
-  DI_CUDA(cudaMemcpy(dc, c, (L + 1) * poly * 4, cudaMemcpyHostToDevice));
+  DI_CUDA(d.stage.h2d(dc, c, (L + 1) * poly * 4, nullptr));
   DI_CUDA(cudaMemcpy(dy, y, R * L * 4, cudaMemcpyHostToDevice));
-  DI_CUDA(cudaMemcpy(dk, sk_y, R * poly * 4, cudaMemcpyHostToDevice));
+  DI_CUDA(d.stage.h2d(dk, sk_y, R * poly * 4, nullptr));
   DI_CHECK(cufe_decrypt(d.ctx, 1, dc, repeat, dy, 0, dk, dd, nullptr));
   DI_CHECK(cufe_sync(d.ctx, nullptr));
-  DI_CUDA(cudaMemcpy(d_y, dd, R * poly * 4, cudaMemcpyDeviceToHost));
+  DI_CUDA(d.stage.d2h(d_y, dd, R * poly * 4, nullptr));
 }
 
 }  // extern "C"

@@ -356,3 +356,44 @@ def test_dropin_abi(rng, oracle_built):
         rdy = O.decrypt(ct[0], y[k], rsk)
         assert (dy[k] == canon(rdy)).all()
         assert int(O.decode(rdy)[0]) == int(x[0].astype(np.int64) @ y[k].astype(np.int64))
+
+
+def test_dropin_staged_copies(rng, oracle_built):
+    """the drop-in symbols at sizes that take the pinned, chunked host copies (mpk and msk
+    of 9.8 MB, two ciphertexts of 19.7 MB: ragged last chunks), against the context API on
+    device buffers with the same seeds"""
+    n, l = 2048, 400
+    L = cf.lib()
+    assert L.cufe_dropin_configure(n, l, 0) == 0
+    s2, s3 = seeds(rng, 2)
+    a = rng.integers(0, 2**31, (3, n), dtype=np.uint64) % np.array(cf.Q, np.uint64)[:, None]
+    mpk = np.zeros((l + 1, 3, n), np.uint32)
+    msk = np.zeros((l, 3, n), np.uint32)
+    mpk[l] = a.astype(np.uint32)
+    L.rlwe_sife_setup_gpu(mpk.ctypes.data, msk.ctypes.data, s2.ctypes.data, s3.ctypes.data, None)
+    assert L.cufe_dropin_status() == 0
+    c = cf.Context(n, l)
+    dmpk, dmsk = c.setup_gpu_map(a.astype(np.uint32), s2, s3)
+    c.sync()
+    assert (mpk == cf.u32(dmpk)).all() and (msk == cf.u32(dmsk)).all()
+    rep = 2
+    x = rng.integers(0, 5, (rep, l), dtype=np.uint32)
+    ct = np.zeros((rep, l + 1, 3, n), np.uint32)
+    L.rlwe_sife_encrypt_gpu(x.ctypes.data, mpk.ctypes.data, ct.ctypes.data, s2.ctypes.data, s2.ctypes.data, rep, None)
+    assert L.cufe_dropin_status() == 0
+    dct = c.encrypt_gpu_map(dev(x), dmpk, s2)
+    y = rng.integers(0, 17, (2, l), dtype=np.uint32)
+    sk = np.zeros((2, 3, n), np.uint32)
+    L.rlwe_sife_keygen_gpu(y.ctypes.data, msk.ctypes.data, sk.ctypes.data, 2, None)
+    dy = np.zeros((2, 3, n), np.uint32)
+    L.rlwe_sife_decrypt_gmp_gpu(ct[1].ctypes.data, y.ctypes.data, sk.ctypes.data, dy.ctypes.data, 2, None)
+    assert L.cufe_dropin_status() == 0
+    dsk = c.keygen(dev(y), dmsk)
+    ddy = c.decrypt(dct[1:2], dev(y), dsk)
+    c.sync()
+    assert (ct == cf.u32(dct)).all()
+    assert (sk == cf.u32(dsk)).all()
+    assert (dy == cf.u32(ddy)[0]).all()
+    dec = cf.u32(c.decode(ddy, ncoeff=1)).reshape(2)
+    assert (dec.astype(np.int64) == (x[1].astype(np.int64) @ y.T.astype(np.int64))).all()
+    c.close()
