@@ -55,7 +55,7 @@ struct Ctx {
 int ntt_launch(const RingArgs &ra, uint32_t *data, long long nres, bool inverse, cudaStream_t s);
 int ntt_fwd_shoup_launch(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s);
 // times the NTT variants on npoly scratch polynomials, keeps the fastest per direction in
-// r.args; ms[4] (optional): {fwd v1, fwd v2, inv v1, inv v2}
+// r.args; ms[2 * CUFE_NTT_VARIANTS] (optional): {fwd v1.., inv v1..} in ms per launch
 int ring_tune(Ring &r, long long npoly, float *ms, cudaStream_t s);
 
 int ctx_setup_cpu_map(Ctx &c, const uint8_t *seed_a, const uint8_t *seed_s, const uint8_t *seed_e, uint32_t *d_mpk,

@@ -29,7 +29,7 @@ struct RingArgs {
   uint32_t w1n[kMaxModuli], w1n_sh[kMaxModuli];    // psi_inv[1] * n^-1 (last inverse stage)
   uint32_t qr[kMaxModuli];                          // floor(2^32 / q)
   const uint2 *psi2, *ipsi2;                       // [k][n] (w, w_shoup) each
-  int pp_fwd, pp_inv;  // NTT kernel variant per direction (1..6), set by the tuner
+  int pp_fwd, pp_inv;  // NTT kernel variant per direction (1..CUFE_NTT_VARIANTS), set by the tuner
 };
 
 // ------------------------------------------------------------------ arithmetic
