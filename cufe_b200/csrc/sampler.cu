@@ -540,8 +540,11 @@ __device__ __forceinline__ void chain_blocks(uint32_t *buf, int from, int to, ui
   }
 }
 
+// 512 threads: the 128 KB of tables allow one CTA per SM, and the chained blocks leave one
+// thread little independent work, so the CTA brings as many warps as the register file holds
+constexpr int kGpuMapThreads = 512;
 template <int SIG>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kGpuMapThreads, 1)
     k_gauss_gpu_map(const uint32_t *__restrict__ rkey, uint32_t poly0, uint32_t npolys, uint32_t n, double kinv,
                     ModArgs m, uint32_t *__restrict__ out, uint32_t *__restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -983,15 +986,18 @@ int sample_cpu_map(int sig, uint32_t nstreams, const uint32_t *d_rkeys, uint32_t
 int sample_gpu_map(int sig, const uint32_t *d_rkey, uint32_t poly0, uint32_t npolys, uint32_t n, uint32_t *d_out,
                    uint32_t *d_status, cudaStream_t s) {
   const uint32_t threads = npolys * (n / 8);
-  const uint32_t grid = (threads + 255) / 256;
+  const uint32_t grid = (threads + kGpuMapThreads - 1) / kGpuMapThreads;
   const double kinv = kinv_of(sig);
   ProfScope ps("sample_gpu_map", s);
   if (sig == 0)
-    note_launch(), k_gauss_gpu_map<0><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<0><<<grid, kGpuMapThreads, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv,
+                                                                               mod_args(), d_out, d_status);
   else if (sig == 1)
-    note_launch(), k_gauss_gpu_map<1><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<1><<<grid, kGpuMapThreads, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv,
+                                                                               mod_args(), d_out, d_status);
   else
-    note_launch(), k_gauss_gpu_map<2><<<grid, 256, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv, mod_args(), d_out, d_status);
+    note_launch(), k_gauss_gpu_map<2><<<grid, kGpuMapThreads, kAesSmemBytes, s>>>(d_rkey, poly0, npolys, n, kinv,
+                                                                               mod_args(), d_out, d_status);
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
 }
