@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(512)
   const uint32_t j = local / 3, l = I.l;
   const int m = (int)(local - j * 3);
   const uint32_t q = ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * P::SMEM_WORDS;
   uint32_t a[16], w[16], wsh[16];
   load16(keys + I.mpk + (size_t)local * P::N + th * 16, a);
   load16(rh + I.rh + (size_t)m * P::N + th * 16, w);
@@ -524,7 +524,7 @@ int Batch::run(cudaStream_t s) {
           attr = true;
         }
         ProfScope ps("batch_encrypt", s);
-        note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, s>>>(
+        note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::SMEM_WORDS * 4, s>>>(
             reinterpret_cast<const InstDev *>(tables + g.inst_off), reinterpret_cast<const uint64_t *>(tables + g.res_off),
             g.count, g.nres, keys, rh, rhsh, f3, s2o, x, ct, ra, mq);
         CUFE_CUDA(cudaGetLastError());
@@ -1001,7 +1001,7 @@ struct Server {
             attr = true;
           }
           ProfScope ps("serve_encrypt", stream);
-          note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::N * 4, stream>>>(
+          note_launch(), k_encrypt_het<LOGN><<<(unsigned)((g.nres + G - 1) / G), dim3(P::T, G), G * P::SMEM_WORDS * 4, stream>>>(
               reinterpret_cast<const InstDev *>(d_tab + g.inst_off), reinterpret_cast<const uint64_t *>(d_tab + g.res_off),
               g.count, g.nres, tenants.keys, rh, rhsh, f3, s2o, xd, d_ct, ra, tenants.mq);
           CUFE_CUDA(cudaGetLastError());

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(LBT, MINB)
   const int m = sel.m[gg % nm];
   const long long row0 = gg / nm * PP;
   const uint32_t q = ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::SMEM_WORDS;
   long long res[PP];
   bool live[PP];
 #pragma unroll
@@ -250,7 +250,7 @@ int launch_ntt_sel(const RingArgs &ra, const ModSel &sel, uint32_t *data, uint32
                    cudaStream_t s) {
   using P = NttPlan<LOGN, LE>;
   constexpr int G = ppc<LOGN, LE>();
-  const size_t smem = (size_t)G * PP * P::N * 4;
+  const size_t smem = (size_t)G * PP * P::SMEM_WORDS * 4;
   static bool attr = false;
   if (!attr) {
     CUFE_CUDA(cudaFuncSetAttribute(k_ntt<LOGN, MODE, PP, LBT, MINB, LE, SQ>,
@@ -292,7 +292,7 @@ __global__ void __maxnreg__(80) k_ntt_stream(uint32_t *__restrict__ data, uint32
   using P = NttPlan<LOGN>;
   extern __shared__ uint32_t smem_u32[];
   const int th = threadIdx.x;
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * P::SMEM_WORDS;
   const long long stride = (long long)gridDim.x * blockDim.y;
   const long long cta0 = (long long)blockIdx.x * blockDim.y;
   const long long iters = cta0 < nres ? (nres - cta0 + stride - 1) / stride : 0;
@@ -363,7 +363,7 @@ template <int LOGN, int MODE>
 int launch_ntt_stream(const RingArgs &ra, uint32_t *data, uint32_t *sh, long long nres, cudaStream_t s) {
   using P = NttPlan<LOGN>;
   constexpr int G = ppc<LOGN>();
-  const size_t smem = (size_t)G * P::N * 4;
+  const size_t smem = (size_t)G * P::SMEM_WORDS * 4;
   static int occ = 0;
   if (!occ) {
     CUFE_CUDA(cudaFuncSetAttribute(k_ntt_stream<LOGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(512) k_setup_mpk(const uint32_t *__restrict__ 
   const long long rr = act ? r : nres - 1;
   const int m = (int)(rr % 3);
   const uint32_t q = ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * P::SMEM_WORDS;
   uint32_t a[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) a[e] = msk[rr * P::N + P::template idx<0>(th, e)];
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T * ppc<LOGN>(), MINB)
   const int b0 = (int)(ww - res * bgroups) * PP;
   const int m = (int)(res % 3), i = (int)(res / 3);
   const uint32_t q = sa.ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * PP * P::SMEM_WORDS;
   uint32_t a[PP][16];
   {
     uint32_t pk[16];
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(512)
   const long long ck = ww / 3;
   const int key = (int)(ck % nkeys), c = (int)(ck / nkeys);
   const uint32_t q = sa.ra.q[m];
-  uint32_t *sm = smem_u32 + threadIdx.y * P::N;
+  uint32_t *sm = smem_u32 + threadIdx.y * P::SMEM_WORDS;
   uint32_t a[16], w[16], wsh[16];
   load16(clhat + ((size_t)c * 3 + m) * P::N + th * 16, a);
   load16(skhat + ((size_t)key * 3 + m) * P::N + th * 16, w);
@@ -968,7 +968,7 @@ static int setup_tail(Ctx &c, int l, uint32_t *d_mpk, const uint32_t *d_msk, uin
     constexpr int G = ppc<LOGN>();
     CUFE_CUDA(cudaFuncSetAttribute(k_setup_mpk<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     ProfScope ps("setup_mpk", s);
-    note_launch(), k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+    note_launch(), k_setup_mpk<LOGN><<<(unsigned)((nres + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::SMEM_WORDS * 4, s>>>(
         d_msk, e, ahat, a_sh, d_mpk, nres, c.ring.args);
     CUFE_CUDA(cudaGetLastError());
     return CUFE_OK;
@@ -1041,12 +1041,12 @@ static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *
       auto kern = k_encrypt<LOGN, 2, MINB>;
       const long long nw = (long long)(c.l + 1) * 3 * ((batch + 1) / 2);
       CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-      note_launch(), kern<<<(unsigned)((nw + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * 2 * NttPlan<LOGN>::N * 4, s>>>(
+      note_launch(), kern<<<(unsigned)((nw + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * 2 * NttPlan<LOGN>::SMEM_WORDS * 4, s>>>(
           d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nw, sa);
     } else {
       auto kern = k_encrypt<LOGN, 1, MINB>;
       CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-      note_launch(), kern<<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::N * 4, s>>>(
+      note_launch(), kern<<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), G * NttPlan<LOGN>::SMEM_WORDS * 4, s>>>(
           d_mpk, rhat, rhat_sh, rhat_stride, f3, f3_stride, f0, f0_stride, d_x, d_ct, batch, nwork, sa);
     }
     CUFE_CUDA(cudaGetLastError());
@@ -1173,7 +1173,7 @@ int ctx_decrypt(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t
   return dispatch_logn(c.ring.logn, [&](auto L) {
     constexpr int LOGN = decltype(L)::value;
     constexpr int G = ppc<LOGN>();
-    const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
+    const size_t smem = (size_t)G * NttPlan<LOGN>::SMEM_WORDS * 4;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     ProfScope ps("decrypt_tail", s);
     note_launch(), k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
@@ -1268,7 +1268,7 @@ int ctx_decrypt_noalloc(Ctx &c, const uint32_t *d_ct, int nkeys, const uint32_t 
   return dispatch_logn(c.ring.logn, [&](auto L) {
     constexpr int LOGN = decltype(L)::value;
     constexpr int G = ppc<LOGN>();
-    const size_t smem = (size_t)G * NttPlan<LOGN>::N * 4;
+    const size_t smem = (size_t)G * NttPlan<LOGN>::SMEM_WORDS * 4;
     CUFE_CUDA(cudaFuncSetAttribute(k_dec_tail<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     note_launch(), k_dec_tail<LOGN><<<(unsigned)((nwork + G - 1) / G), dim3(NttPlan<LOGN>::T, G), smem, s>>>(
         part, nsplit, clhat, skhat, skhat_sh, nkeys, d_dy, nwork, sa);

@@ -9,9 +9,10 @@
 // registers (E = 16 everywhere; the batched transform kernel also has E = 32 and 64 forms,
 // picked by the ring's tuner).  The log2(n) butterfly stages are grouped into passes of up
 // to LE stages (radix E); a pass touches only the E coefficients of a thread, and consecutive passes
-// exchange coefficients through shared memory (one __syncthreads per exchange) with an
-// XOR swizzle (j ^ ((j >> s) & 31), s = 4 for radix 16 and LE otherwise) that keeps every
-// exchange pattern of these plans free of bank conflicts without padding.  The smaller pass
+// exchange coefficients through shared memory (one __syncthreads per exchange), one padding
+// word per 32 (64 for radix 64) and, in the middle radix-16 pass, thread bits 4 and 5
+// swapped: every exchange pattern of these plans is free of bank conflicts (n >= 1024) and
+// every address is a per-thread base plus an immediate.  The smaller pass
 // (log2(n) mod LE stages) comes first so that the strided passes are the early ones, whose
 // warps touch 32 consecutive words.  Twiddles use Shoup's precomputed quotient (1 mul.hi +
 // 2 mul.lo per product) and residues stay canonical in [0, q), q < 2^31, between kernels.
@@ -28,18 +29,35 @@ struct NttPlan {
   static constexpr int T = N / E;  // threads per residue polynomial
   static constexpr int NP = (LOGN + LE - 1) / LE;
   static constexpr int R0 = LOGN - LE * (NP - 1);
-  static constexpr int SMEM_WORDS = N;
+  // shared-memory layout of an exchange: coefficient j at word pad(j) = j + (j >> PADS), one
+  // padding word per 2^PADS.  pad is additive over disjoint bits, so a thread's address of
+  // register e is pad(idx_th) + pad(idx_e): a per-thread base plus an immediate offset.
+  static constexpr int PADS = LE == 6 ? 6 : 5;
+  static constexpr int SMEM_WORDS = N + (N >> PADS);
+  __host__ __device__ static constexpr int pad(int j) { return j + (j >> PADS); }
   __host__ __device__ static constexpr int radix_bits(int p) { return p == 0 ? R0 : LE; }
   __host__ __device__ static constexpr int first_stage(int p) { return p == 0 ? 0 : R0 + LE * (p - 1); }
+  // A radix-16 pass whose warp lanes would cover index bits 0..3 and 8 (the middle passes:
+  // thread bits below position 4, the rest above the pass's 4 register bits) takes thread
+  // bit 5 in place of bit 4, so its fifth lane bit lands on index bit 9, whose padded weight
+  // (512 + 16) completes the bank set of bits 0..3; every exchange is then conflict-free.
+  __host__ __device__ static constexpr bool lane_swap(int p) {
+    return LE == 4 && LOGN - first_stage(p) - radix_bits(p) == 4 && T >= 64;
+  }
+  template <int PASS>
+  __host__ __device__ static constexpr int vth(int th) {
+    return lane_swap(PASS) ? ((th & ~0x30) | ((th >> 1) & 0x10) | ((th << 1) & 0x20)) : th;
+  }
   // coefficient index held in register e by thread th during pass PASS.  The bits that come
   // from th and the bits that come from e are disjoint, so idx = idx_th(th) + idx_e(e), the
   // second a compile-time constant (an immediate offset in every load and store).  A pass
   // of rb < LE stages runs E >> rb butterfly blocks per thread ("virtual threads" v*T + th).
   template <int PASS>
-  __device__ __forceinline__ static int idx_th(int th) {
+  __host__ __device__ static constexpr int idx_th(int th) {
     constexpr int rb = radix_bits(PASS), s0 = first_stage(PASS);
     constexpr int plo = LOGN - s0 - rb, phi = LOGN - 1 - s0;
-    return ((th >> plo) << (phi + 1)) | (th & ((1 << plo) - 1));
+    const int t = vth<PASS>(th);
+    return ((t >> plo) << (phi + 1)) | (t & ((1 << plo) - 1));
   }
   template <int PASS>
   __host__ __device__ static constexpr int idx_e(int e) {
@@ -51,34 +69,28 @@ struct NttPlan {
   __device__ __forceinline__ static int idx(int th, int e) {
     return idx_th<PASS>(th) + idx_e<PASS>(e);
   }
-  // XOR swizzle: bits LE..LE+4 of the index folded into the bank bits.  The lanes of a warp
-  // cover index bits 0..4 in the early passes and bits LE..LE+4 in the last one; the fold
-  // keeps both (and, for LE = 4, the middle pass's bits 0..3 + 8) conflict-free.
-  __host__ __device__ static constexpr int swz(int j) { return j ^ ((j >> (LE == 4 ? 4 : LE)) & 31); }
+  static_assert(pad(N - 1) < SMEM_WORDS, "exchange layout");
 };
 
 // P residue polynomials per thread group (same modulus, shared twiddles and addresses):
-// polynomial p uses registers a[p][] and shared words sm[p * N ...]
-// The swizzle is linear over XOR and idx_th / idx_e have disjoint bits, so the swizzled
-// address of register e is swz(idx_th(th)) ^ swz(idx_e(e)): one per-thread base and one XOR
-// with a constant per access.
+// polynomial p uses registers a[p][] and shared words sm[p * SMEM_WORDS ...]; every address is
+// one per-thread base plus a compile-time offset (pad is additive over the disjoint bits of
+// idx_th and idx_e).
 template <int LOGN, int FROM, int TO, int P_, int LE, int E>
 __device__ __forceinline__ void ntt_exchange(uint32_t (&a)[P_][E], uint32_t *sm, int th) {
   using P = NttPlan<LOGN, LE>;
-  const int wb = P::swz(P::template idx_th<FROM>(th));
+  uint32_t *wb = sm + P::pad(P::template idx_th<FROM>(th));
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    const int j = wb ^ P::swz(P::template idx_e<FROM>(e));
 #pragma unroll
-    for (int p = 0; p < P_; ++p) sm[p * P::N + j] = a[p][e];
+    for (int p = 0; p < P_; ++p) wb[p * P::SMEM_WORDS + P::pad(P::template idx_e<FROM>(e))] = a[p][e];
   }
   __syncthreads();
-  const int rbase = P::swz(P::template idx_th<TO>(th));
+  const uint32_t *rb = sm + P::pad(P::template idx_th<TO>(th));
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    const int j = rbase ^ P::swz(P::template idx_e<TO>(e));
 #pragma unroll
-    for (int p = 0; p < P_; ++p) a[p][e] = sm[p * P::N + j];
+    for (int p = 0; p < P_; ++p) a[p][e] = rb[p * P::SMEM_WORDS + P::pad(P::template idx_e<TO>(e))];
   }
 }
 
@@ -124,7 +136,7 @@ __device__ __forceinline__ void ntt_stage(uint32_t (&a)[P_][E], int th, uint32_t
   constexpr int s = s0 + LS, half = 1 << (rb - 1 - LS), nv = E >> rb, ng = 1 << LS;
 #pragma unroll
   for (int v = 0; v < nv; ++v) {
-    const int H = (v * P::T + th) >> plo;
+    const int H = (v * P::T + P::template vth<PASS>(th)) >> plo;
     if constexpr (INV && s == 0) {
 #pragma unroll
       for (int b = 0; b < half; ++b) {

@@ -6,9 +6,12 @@ restated in Python and checked on the CPU for every ring size and radix the kern
   lets the kernels address register e with a compile-time offset;
 - a pass of rb stages pairs, in its stage LS, registers that differ only in the butterfly
   bit of that stage (a radix-2^rb block is held by one thread);
-- every exchange between passes is free of shared-memory bank conflicts under the XOR
-  swizzle, for the stores of the pass that ends and the loads of the pass that begins (one
-  warp = 32 consecutive threads of a residue group).
+- the shared-memory layout pad(j) = j + (j >> s) (s = 6 for radix 64, else 5) is injective,
+  fits SMEM_WORDS and is additive over the disjoint thread and register bits (so an address
+  is a per-thread base plus an immediate);
+- with thread bits 4 and 5 swapped in the middle radix-16 passes, every exchange between
+  passes is free of shared-memory bank conflicts, for the stores of the pass that ends and
+  the loads of the pass that begins (one warp = 32 consecutive threads of a residue group).
 """
 from collections import Counter
 
@@ -30,7 +33,16 @@ class Plan:
     def s0(self, p):
         return 0 if p == 0 else self.R0 + self.le * (p - 1)
 
+    def lane_swap(self, p):
+        return self.le == 4 and self.logn - self.s0(p) - self.rb(p) == 4 and self.T >= 64
+
+    def vth(self, p, th):
+        if not self.lane_swap(p):
+            return th
+        return (th & ~0x30) | (((th >> 5) & 1) << 4) | (((th >> 4) & 1) << 5)
+
     def idx_th(self, p, th):
+        th = self.vth(p, th)
         plo, phi = self.logn - self.s0(p) - self.rb(p), self.logn - 1 - self.s0(p)
         return ((th >> plo) << (phi + 1)) | (th & ((1 << plo) - 1))
 
@@ -40,8 +52,11 @@ class Plan:
         v = (e >> rb) * self.T
         return ((v >> plo) << (phi + 1)) | ((e & ((1 << rb) - 1)) << plo) | (v & ((1 << plo) - 1))
 
-    def swz(self, j):
-        return j ^ ((j >> (4 if self.le == 4 else self.le)) & 31)
+    def pad(self, j):
+        return j + (j >> (6 if self.le == 6 else 5))
+
+    def smem_words(self):
+        return self.N + (self.N >> (6 if self.le == 6 else 5))
 
 
 # (log n, log2 coefficients per thread) of every k_ntt instantiation: radix 16 for all rings,
@@ -78,11 +93,24 @@ def test_plan_stage_pairs(logn, le):
                 assert P.idx_e(p, e1) ^ P.idx_e(p, e1 + half) == 1 << bit
 
 
-@pytest.mark.parametrize("logn,le", [pl for pl in PLANS if Plan(*pl).T >= 32])
+@pytest.mark.parametrize("logn,le", PLANS)
+def test_layout_injective_additive(logn, le):
+    P = Plan(logn, le)
+    img = [P.pad(j) for j in range(P.N)]
+    assert len(set(img)) == P.N and max(img) < P.smem_words()
+    for p in range(P.NP):
+        for th in range(P.T):
+            a = P.idx_th(p, th)
+            for e in range(P.E):
+                b = P.idx_e(p, e)
+                assert P.pad(a + b) == P.pad(a) + P.pad(b)
+
+
+@pytest.mark.parametrize("logn,le", [pl for pl in PLANS if Plan(*pl).logn >= 10])
 def test_exchanges_conflict_free(logn, le):
     P = Plan(logn, le)
     for p in range(P.NP):
         for e in range(P.E):
             for w0 in range(0, P.T, 32):
-                banks = Counter(P.swz(P.idx_th(p, th) + P.idx_e(p, e)) % 32 for th in range(w0, w0 + 32))
+                banks = Counter(P.pad(P.idx_th(p, th) + P.idx_e(p, e)) % 32 for th in range(w0, w0 + 32))
                 assert max(banks.values()) == 1, (logn, le, p, e, w0)
