@@ -204,12 +204,26 @@ __global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ 
   const uint64_t r0 = __ldg(sg.roff + st), R = __ldg(sg.roff + st + 1) - r0;
   const uint64_t base = (uint64_t)(T - __ldg(sg.toff + st)) * kScanTile + threadIdx.x * 8;
   uint32_t cnt[8], tot = 0;
+  // whole runs at 8-byte aligned masks and 16-byte aligned prefixes (every refill range of a
+  // uniform table in the 256-byte aligned scratch): one 8-byte load, two 16-byte stores
+  const bool vec = base + 8 <= R && (reinterpret_cast<uintptr_t>(amask + r0 + base) & 7u) == 0 &&
+                   (reinterpret_cast<uintptr_t>(elocal + r0 + base) & 15u) == 0;
+  if (vec) {
+    const uint2 m8 = __ldg(reinterpret_cast<const uint2 *>(amask + r0 + base));
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const uint64_t t = base + i;
-    cnt[i] = t < R ? __popc(amask[r0 + t]) : 0u;
-    tot += cnt[i];
+    for (int i = 0; i < 4; ++i) {
+      cnt[i] = __popc((m8.x >> (8 * i)) & 0xffu);
+      cnt[4 + i] = __popc((m8.y >> (8 * i)) & 0xffu);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t t = base + i;
+      cnt[i] = t < R ? __popc(amask[r0 + t]) : 0u;
+    }
   }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) tot += cnt[i];
   // block exclusive scan of per-thread totals
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t inc = tot;
@@ -232,11 +246,20 @@ __global__ void __launch_bounds__(512) k_scan_tiles(const uint8_t *__restrict__ 
   }
   __syncthreads();
   uint32_t run = wsum[wid] + inc - tot;
+  uint32_t ex[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const uint64_t t = base + i;
-    if (t < R) elocal[r0 + t] = run;
+    ex[i] = run;
     run += cnt[i];
+  }
+  if (vec) {
+    uint4 *o = reinterpret_cast<uint4 *>(elocal + r0 + base);
+    o[0] = make_uint4(ex[0], ex[1], ex[2], ex[3]);
+    o[1] = make_uint4(ex[4], ex[5], ex[6], ex[7]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (base + i < R) elocal[r0 + base + i] = ex[i];
   }
 }
 
