@@ -1,16 +1,22 @@
 // staging.cpp -- see staging.h.
 #include "staging.h"
 
+#include <unistd.h>
+
 #include <algorithm>
 #include <cstring>
 
 namespace cufe {
 
-CopyPool::CopyPool(int nthreads) : n_(std::max(1, nthreads)) {
+CopyPool::CopyPool(int nthreads) : n_(std::max(1, nthreads)), pid_((long)getpid()) {
   for (int i = 1; i < n_; ++i) th_.emplace_back(&CopyPool::worker, this, i);
 }
 
 CopyPool::~CopyPool() {
+  if ((long)getpid() != pid_) {  // a fork()ed child: the workers live in the parent only
+    for (auto &t : th_) t.detach();
+    return;
+  }
   {
     std::lock_guard<std::mutex> lk(mu_);
     stop_ = true;
@@ -49,7 +55,7 @@ void CopyPool::worker(int id) {
 }
 
 void CopyPool::copy(void *dst, const void *src, size_t bytes) {
-  if (n_ == 1 || bytes < ((size_t)1 << 20)) {
+  if (n_ == 1 || bytes < ((size_t)1 << 20) || (long)getpid() != pid_) {
     std::memcpy(dst, src, bytes);
     return;
   }

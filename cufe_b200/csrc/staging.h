@@ -31,6 +31,7 @@ class CopyPool {
   void worker(int id);
   void slice(int id, char *dst, const char *src, size_t bytes) const;
   int n_;
+  long pid_;  // the process whose threads these are (a fork()ed child copies alone)
   std::vector<std::thread> th_;
   std::mutex mu_;
   std::condition_variable cv_, done_cv_;
