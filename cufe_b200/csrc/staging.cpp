@@ -13,8 +13,8 @@ CopyPool::CopyPool(int nthreads) : n_(std::max(1, nthreads)), pid_((long)getpid(
 }
 
 CopyPool::~CopyPool() {
-  if ((long)getpid() != pid_) {  // a fork()ed child: the workers live in the parent only
-    for (auto &t : th_) t.detach();
+  if ((long)getpid() != pid_) {  // a fork()ed child: the workers live in the parent only, so
+    new std::vector<std::thread>(std::move(th_));  // their handles are left alone (leaked)
     return;
   }
   {
