@@ -207,18 +207,18 @@ def cpu_baseline_sample(x, y, seeds2, setup_seeds, nproc, steps=2):
 # ----------------------------------------------------------------------------- GPU arm
 
 # DRAM bytes per refill of the sigma_3 candidate kernel, from one ncu capture of a batch-16
-# launch (dram__bytes_read.sum + dram__bytes_write.sum = 0.26 MB + 1301.44 MB over
+# launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.49 MB + 676.2 MB over
 # 16 x 1,103,616 refills); traffic grows with the refill count, so a launch of B streams
 # moves B x refills x this
-CAND_S3_DRAM_BYTES_PER_REFILL = (0.257792e6 + 1301.437e6) / (16 * 1103616)
+CAND_S3_DRAM_BYTES_PER_REFILL = (1.494528e6 + 676.216064e6) / (16 * 1103616)
 
 
 # algorithmic HBM bytes per launch of each kernel at this workload (batch B)
 def algorithmic_bytes(kernel, B, refills3):
     poly = 3 * N * 4
     return {
-        "sample_cand_s3": refills3 * B * 65,           # 8 x int64 candidates + accept mask
-        "sample_scatter": refills3 * B * 65 + B * L * poly,  # candidates and masks; f_i residues
+        "sample_cand_s3": refills3 * B * 35,           # 8 low words, accept mask, bit-32/sign bytes
+        "sample_scatter": refills3 * B * 35 + B * L * poly,  # candidates and masks; f_i residues
         "encrypt_intt": (L + 1) * poly + B * (L * poly + (L + 1) * poly),  # mpk once, f_i, ciphertexts
         "decrypt_mac": B * (L + 1) * poly + B * poly,    # ciphertexts read, partial sums written
         "decode": B * poly + B * N * 4,

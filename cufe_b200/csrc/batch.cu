@@ -732,7 +732,9 @@ struct Server {
   static uint64_t enc_scratch_bytes(uint32_t n, uint32_t l) {
     const uint64_t poly = (uint64_t)3 * n * 4;
     const uint64_t R3 = cpu_map_refills(l, n, 2), R2 = cpu_map_refills(2, n, 1);
-    return poly * (2 + 2 + l) + std::max(R3, R2) * 70 + 2 * 60 * 4 + 8192;
+    // sampler scratch: 39 B per refill (candidate low words 32, accept mask 1, bit-32 and sign
+    // bytes 2, prefix 4) plus tiles and call starts; 44 leaves room for the per-tile terms
+    return poly * (2 + 2 + l) + std::max(R3, R2) * 44 + 2 * 60 * 4 + 8192;
   }
 
   void retire(Tick &t) {

@@ -111,8 +111,8 @@ constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed
 
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)
-    k_cand_cpu(const uint32_t *__restrict__ rkeys, SegDev sg, double kinv, int64_t *__restrict__ cand,
-               uint8_t *__restrict__ amask, uint32_t *__restrict__ status) {
+    k_cand_cpu(const uint32_t *__restrict__ rkeys, SegDev sg, double kinv, uint32_t *__restrict__ cand_lo,
+               uint8_t *__restrict__ amask, uint16_t *__restrict__ chs, uint32_t *__restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
   aes_fill_tables(smem);
   __syncthreads();
@@ -164,9 +164,10 @@ __global__ void __launch_bounds__(kCandThreads, 1)
 #pragma unroll
     for (int j = 0; j < 8; ++j) ybuf[j] = y[j];
     const uint32_t k8 = bswap32(buf[kbuf(70)]) & 0xffu;  // sign byte 280
-    // 3. the 8 candidates, one code copy
-    uint32_t acc = 0;
-    int64_t v8[8];
+    // 3. the 8 candidates, one code copy: |value| = z < 8K < 2^33 as its low word, bit 32 and
+    // the sign byte
+    uint32_t acc = 0, hib = 0, wide = 0;
+    uint32_t lo8[8];
 #pragma unroll 1
     for (int ln = 0; ln < 8; ++ln) {
       const int h = ln >> 2, li = ln & 3;
@@ -180,13 +181,18 @@ __global__ void __launch_bounds__(kCandThreads, 1)
       uint64_t z;
       const bool b = candidate<SIG, VAR>(x, ybuf[ln], rm, rexp, kinv, z);
       const uint32_t k = (k8 >> ln) & 1u;
-      acc |= (uint32_t)accept_final(b, z, k) << ln;
-      v8[ln] = k ? -(int64_t)z : (int64_t)z;
+      const uint32_t a = accept_final(b, z, k);
+      acc |= a << ln;
+      lo8[ln] = (uint32_t)z;
+      hib |= (uint32_t)((z >> 32) & 1u) << ln;
+      wide |= a & (uint32_t)((z >> 33) != 0);
     }
-    longlong2 *dst = reinterpret_cast<longlong2 *>(cand + (size_t)g * 8);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dst[i] = make_longlong2(v8[2 * i], v8[2 * i + 1]);
+    uint4 *dst = reinterpret_cast<uint4 *>(cand_lo + (size_t)g * 8);
+    dst[0] = make_uint4(lo8[0], lo8[1], lo8[2], lo8[3]);
+    dst[1] = make_uint4(lo8[4], lo8[5], lo8[6], lo8[7]);
     amask[g] = (uint8_t)acc;
+    chs[g] = (uint16_t)(hib | (k8 << 8));
+    if (wide) atomicOr(status, kStatusWideSample);
   }
 }
 
@@ -470,21 +476,31 @@ __device__ __forceinline__ uint32_t signed_residue(int64_t s, const ModArgs &m, 
   return s >= 0 || r == 0 ? r : q - r;
 }
 
+// (-1)^neg (hi 2^32 + lo) mod q_j for hi <= 1: lo mod q by one multiply-high (lo -
+// floor(lo qr / 2^32) q is in [0, 2q)), plus 2^32 mod q when hi is set
+__device__ __forceinline__ uint32_t residue_parts(uint32_t lo, uint32_t hi, uint32_t neg, const ModArgs &m, int j) {
+  const uint32_t q = m.q[j];
+  uint32_t r = mod_red1(lo - __umulhi(lo, m.qr[j]) * q, q);
+  if (hi) r = mod_add(r, m.c32[j], q);
+  return neg && r ? q - r : r;
+}
+
 // one CTA per call of the flattened call space: the accepted candidates of refills
 // [a_c, a_{c+1}) in order, as residues out[ooff[st] + c * 3n ...][3][n].  Warp w of the CTA
-// takes a contiguous run of the call's refills, 32 at a time: lane L loads the accept mask of
-// refill t + L and, for k = 0..7, candidate L & 7 of refill t + 4k + L / 8 (eight coalesced
-// 256-byte loads in flight per warp).  Per k the warp ballots the accepted lanes and packs
+// takes a contiguous run of the call's refills, 32 at a time: lane L loads the accept, bit-32
+// and sign bits of refill t + L and, for k = 0..7, the low word of candidate L & 7 of refill
+// t + 4k + L / 8 (eight coalesced 128-byte loads in flight per warp).  Per k the warp ballots the accepted lanes and packs
 // them, in refill order and then candidate order (the order the reference consumes them), into
 // a per-warp staging array; then every lane reduces one staged sample and the warp writes
 // consecutive output positions.  Only the first position of each warp's run comes from the
 // prefix tables.
 constexpr int kScatterThreads = 256;
 __global__ void __launch_bounds__(kScatterThreads)
-    k_scatter(const int64_t *__restrict__ cand, const uint8_t *__restrict__ amask, const uint32_t *__restrict__ elocal,
+    k_scatter(const uint32_t *__restrict__ cand_lo, const uint8_t *__restrict__ amask,
+              const uint16_t *__restrict__ chs, const uint32_t *__restrict__ elocal,
               const uint32_t *__restrict__ tile_off, const uint32_t *__restrict__ call_start, SegDev sg, ModArgs m,
               uint32_t *__restrict__ out) {
-  __shared__ int64_t stage[kScatterThreads / 32][256];
+  __shared__ uint2 stage[kScatterThreads / 32][256];
   const uint32_t st = seg_find(sg.coff, sg.nstreams, blockIdx.x);
   const uint64_t cs0 = __ldg(sg.coff + st);
   const uint32_t c = (uint32_t)(blockIdx.x - cs0);
@@ -500,29 +516,34 @@ __global__ void __launch_bounds__(kScatterThreads)
   const uint32_t t1 = min(t0 + span, b);
   uint32_t pos = prefix_at(elocal, tile_off, amask, v, t0) - prefix_at(elocal, tile_off, amask, v, a);
   uint32_t *o = out + __ldg(sg.ooff + st) + (size_t)c * 3 * n;
-  int64_t *sw = stage[threadIdx.x >> 5];
+  uint2 *sw = stage[threadIdx.x >> 5];
   const uint32_t below = (1u << lane) - 1u, ci = lane & 7u;
   for (uint32_t t = t0; t < t1 && pos < n; t += 32) {
-    const uint32_t mk = t + lane < t1 ? __ldg(amask + v.r0 + t + lane) : 0u;
-    int64_t sv[8];
+    // refill t + lane: accept bits, bit 32 of each |value| (<< 8), signs (<< 16)
+    const uint32_t mk = t + lane < t1 ? (uint32_t)__ldg(amask + v.r0 + t + lane) |
+                                            ((uint32_t)__ldg(chs + v.r0 + t + lane) << 8)
+                                      : 0u;
+    uint32_t lv[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const uint32_t r = t + 4 * k + (lane >> 3);
-      sv[k] = r < t1 ? __ldg(cand + (v.r0 + r) * 8 + ci) : 0;
+      lv[k] = r < t1 ? __ldg(cand_lo + (v.r0 + r) * 8 + ci) : 0u;
     }
     uint32_t cnt = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const bool acc = (__shfl_sync(0xffffffffu, mk, 4 * k + (lane >> 3)) >> ci) & 1u;
+      const uint32_t meta = __shfl_sync(0xffffffffu, mk, 4 * k + (lane >> 3)) >> ci;
+      const bool acc = meta & 1u;
       const uint32_t bal = __ballot_sync(0xffffffffu, acc);
-      if (acc) sw[cnt + __popc(bal & below)] = sv[k];
+      if (acc)  // staged as (low word, bit 32 | sign << 31)
+        sw[cnt + __popc(bal & below)] = make_uint2(lv[k], ((meta >> 8) & 1u) | (((meta >> 16) & 1u) << 31));
       cnt += __popc(bal);
     }
     __syncwarp();
     for (uint32_t i = lane; i < cnt && pos + i < n; i += 32) {
-      const int64_t sval = sw[i];
+      const uint2 sv = sw[i];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) o[j * n + pos + i] = signed_residue(sval, m, j);
+      for (int j = 0; j < 3; ++j) o[j * n + pos + i] = residue_parts(sv.x, sv.y & 1u, sv.y >> 31, m, j);
     }
     __syncwarp();  // the next step overwrites the staging array
     pos += cnt;
@@ -910,7 +931,8 @@ bool seg_auto_doubling(uint64_t refills, uint32_t max_calls) {
 }
 
 size_t seg_scratch_bytes(const SegSizes &z) {
-  size_t b = align256(z.refills * 64) + align256(z.refills) + align256(z.refills * 4) + align256((size_t)z.tiles * 4) +
+  size_t b = align256(z.refills * 32) + align256(z.refills) + align256(z.refills * 2) + align256(z.refills * 4) +
+             align256((size_t)z.tiles * 4) +
              align256((z.calls + z.nstreams) * 4);
   if (z.doubling) b += (size_t)doubling_levels(z.max_calls) * align256(z.refills * 4);
   return b;
@@ -931,8 +953,9 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
     p += align256(x);
     return r;
   };
-  int64_t *cand = reinterpret_cast<int64_t *>(take(z.refills * 64));
+  uint32_t *cand = reinterpret_cast<uint32_t *>(take(z.refills * 32));  // low words of |candidate|
   uint8_t *amask = take(z.refills);
+  uint16_t *chs = reinterpret_cast<uint16_t *>(take(z.refills * 2));  // bit 32 of each, signs << 8
   uint32_t *elocal = reinterpret_cast<uint32_t *>(take(z.refills * 4));
   uint32_t *tsum = reinterpret_cast<uint32_t *>(take((size_t)z.tiles * 4));
   uint32_t *cstart = reinterpret_cast<uint32_t *>(take((z.calls + z.nstreams) * 4));
@@ -942,11 +965,14 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
   if (grid > 0) {
     ProfScope ps(sig == 0 ? "sample_cand_s1" : (sig == 1 ? "sample_cand_s2" : "sample_cand_s3"), s);
     if (sig == 0)
-      note_launch(), k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<0, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, chs,
+                                                                             d_status);
     else if (sig == 1)
-      note_launch(), k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<1, false, 0><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, chs,
+                                                                             d_status);
     else
-      note_launch(), k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, d_status);
+      note_launch(), k_cand_cpu<2, true, 1><<<grid, kCandThreads, kAesSmemBytes, s>>>(d_rkeys, sg, kinv, cand, amask, chs,
+                                                                             d_status);
   }
   CUFE_CUDA(cudaGetLastError());
   if (z.tiles) {
@@ -971,7 +997,8 @@ int sample_cpu_map_seg(int sig, const SegDev &sg, const SegSizes &z, const uint3
   CUFE_CUDA(cudaGetLastError());
   if (d_out && z.calls) {
     ProfScope ps_sc("sample_scatter", s);
-    note_launch(), k_scatter<<<(uint32_t)z.calls, kScatterThreads, 0, s>>>(cand, amask, elocal, tsum, cstart, sg, mod_args(), d_out);
+    note_launch(), k_scatter<<<(uint32_t)z.calls, kScatterThreads, 0, s>>>(cand, amask, chs, elocal, tsum, cstart, sg,
+                                                                           mod_args(), d_out);
     CUFE_CUDA(cudaGetLastError());
   }
   return CUFE_OK;

@@ -31,6 +31,7 @@ enum : uint32_t {
   kStatusUniformOverrun = 1u,   // a uniform draw ran past the 384-byte refill (reference UB)
   kStatusRefillsExhausted = 2u, // mode A: the precomputed refills did not cover all calls
   kStatusRefillCap = 4u,        // GPU mapping: a thread exceeded kMaxRefillsPerThread refills
+  kStatusWideSample = 8u,       // an accepted candidate at or above 2^33 (z = K x + y < 8K keeps it below)
 };
 // refills one GPU-mapping thread may draw for its 8 samples (needs about 2; 64 has
 // probability far below 2^-400 of being exceeded)
