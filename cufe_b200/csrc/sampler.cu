@@ -459,23 +459,6 @@ struct ModArgs {
   uint32_t c32[3];  // 2^32 mod q
 };
 
-// s mod q_j in [0, q_j).  Samples satisfy |s| < 8K < 2^33 (z = K x + y, x <= 7, y < K):
-// |s| = hi 2^32 + lo with hi <= 1, lo mod q by one multiply-high (lo - floor(lo qr / 2^32) q
-// is in [0, 2q)), plus 2^32 mod q when hi = 1; anything wider takes the 64-bit reduction.
-__device__ __forceinline__ uint32_t signed_residue(int64_t s, const ModArgs &m, int j) {
-  const uint64_t u = s >= 0 ? (uint64_t)s : (uint64_t)(-s);
-  const uint32_t q = m.q[j];
-  uint32_t r;
-  if (u < (1ull << 33)) {
-    const uint32_t lo = (uint32_t)u;
-    r = mod_red1(lo - __umulhi(lo, m.qr[j]) * q, q);
-    if (u >> 32) r = mod_add(r, m.c32[j], q);
-  } else {
-    r = mod_u64(u, m.mu[j], q);
-  }
-  return s >= 0 || r == 0 ? r : q - r;
-}
-
 // (-1)^neg (hi 2^32 + lo) mod q_j for hi <= 1: lo mod q by one multiply-high (lo -
 // floor(lo qr / 2^32) q is in [0, 2q)), plus 2^32 mod q when hi is set
 __device__ __forceinline__ uint32_t residue_parts(uint32_t lo, uint32_t hi, uint32_t neg, const ModArgs &m, int j) {
@@ -675,11 +658,12 @@ __global__ void __launch_bounds__(kGpuMapThreads, 1)
       if (accept_final((acc >> (i - 1)) & 1u, z[i - 1], k)) break;
     }
     if (gave_up) break;
-    const int64_t zs = (int64_t)z[i - 1];
-    const int64_t s = k ? -zs : zs;
+    const uint64_t zs = z[i - 1];  // K x + y < 8K < 2^33
+    if (zs >> 33) atomicOr(status, kStatusWideSample);
     const uint32_t pos = 8 * t + j;
 #pragma unroll
-    for (int jj = 0; jj < 3; ++jj) o[jj * n + pos] = signed_residue(s, m, jj);
+    for (int jj = 0; jj < 3; ++jj)
+      o[jj * n + pos] = residue_parts((uint32_t)zs, (uint32_t)(zs >> 32) & 1u, k, m, jj);
   }
 }
 
