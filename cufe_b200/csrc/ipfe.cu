@@ -898,8 +898,12 @@ int Ctx::check_status(cudaStream_t s) {
   CUFE_CUDA(cudaStreamSynchronize(s));
   if (st) {
     CUFE_CUDA(cudaMemsetAsync(d_status, 0, 4, s));
-    set_last_error(std::string("sampler status ") + std::to_string(st) +
-                   ((st & 2) ? " (refill range exhausted)" : " (uniform draw beyond the refill buffer)"));
+    std::string why;
+    if (st & 1u) why += " uniform draw beyond the refill buffer;";
+    if (st & 2u) why += " precomputed refill range exhausted;";
+    if (st & 4u) why += " GPU-mapping refill cap reached;";
+    if (st & 8u) why += " candidate at or above 2^33;";
+    set_last_error(std::string("sampler status ") + std::to_string(st) + ":" + why);
     return CUFE_ERR_SAMPLER;
   }
   return CUFE_OK;
