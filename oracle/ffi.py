@@ -299,3 +299,28 @@ def canon(a, axis_moduli=-2):
     shape = [1] * a.ndim
     shape[axis_moduli] = 3
     return (a % q.reshape(shape)).astype(np.uint32)
+
+
+class ReferenceModeB:
+    """The reference's GPU sampler kernels (src/sample_gpu.cu, src/AES.cuh, src/sampler.cuh) run
+    on the host by oracle/ref/modeb/modeb_host.cpp: one block = one polynomial at n = 4096."""
+
+    def __init__(self):
+        L = _load(os.path.join(HERE, "_ref", "modeb", "libmodeb.so"))
+        L.modeb_block.argtypes = [C.c_int, _u8p, C.c_int, _u32p]
+        L.modeb_prepare_key.argtypes = [_u8p, _u8p]
+        L.modeb_n.restype = C.c_int
+        self.L = L
+        self.n = L.modeb_n()
+
+    def prepare_key(self, seed):
+        rk = np.zeros(240, np.uint8)
+        self.L.modeb_prepare_key(np.ascontiguousarray(seed, np.uint8), rk)
+        return rk
+
+    def poly(self, sig, seed, bid):
+        out = np.zeros(3 * self.n, np.uint32)
+        rc = self.L.modeb_block(sig, np.ascontiguousarray(seed, np.uint8), bid, out)
+        if rc:
+            raise RuntimeError("modeb_block failed: %d" % rc)
+        return out.reshape(3, self.n)

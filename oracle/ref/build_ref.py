@@ -1,5 +1,7 @@
 """Build the reference's own CPU path (cuFE src/*.c, compiled unmodified from where the
-sources lie under /root/reference) into oracle/_ref/<variant>/libref.so.
+sources lie in the reference tree given by --root or $CUFE_REFERENCE_ROOT) into
+oracle/_ref/<variant>/libref.so, and the reference's GPU sampler kernels as host code into
+oracle/_ref/modeb/libmodeb.so.
 
 TEST INFRASTRUCTURE ONLY: the resulting libraries are the pinned oracle that the C
 restatement (oracle/cufe_oracle.c) and the golden fixtures are checked against, and the
@@ -17,6 +19,7 @@ Recipe (no copying of reference sources; outputs only under oracle/_ref/):
     explicit x86-64-v3 target keeps the library runnable on any AVX2 host and keeps
     the FMA contraction of the Bernoulli polynomial that -march=native gives).
 """
+import argparse
 import os
 import subprocess
 import sys
@@ -24,8 +27,6 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT = os.path.join(ORACLE, "_ref")
-REF = os.environ.get("CUFE_REFERENCE_ROOT", "/root/reference")
-SRC = os.path.join(REF, "src")
 UNITS = ["aes256ctr.c", "arith_rns.c", "crt.c", "gauss.c", "ntt.c", "rlwe_sife.c", "sample.c"]
 CFLAGS = ["-O3", "-fomit-frame-pointer", "-march=x86-64-v3", "-maes", "-fPIC", "-w",
           "-ftrivial-auto-var-init=zero"]
@@ -89,7 +90,15 @@ def gen_headers(n, l, d):
         f.write("#endif\n")
 
 
-def build_variant(name, dims, force=False):
+def ref_root(root=None):
+    """the reference tree: the argument, else $CUFE_REFERENCE_ROOT; there is no default"""
+    root = root or os.environ.get("CUFE_REFERENCE_ROOT")
+    if not root:
+        raise RuntimeError("reference tree not given: pass root= / --root or set CUFE_REFERENCE_ROOT")
+    return root
+
+
+def build_variant(root, name, dims, force=False):
     d = os.path.join(OUT, name)
     lib = os.path.join(d, "libref.so")
     if os.path.exists(lib) and not force:
@@ -99,10 +108,11 @@ def build_variant(name, dims, force=False):
     if dims is not None:
         gen_headers(dims[0], dims[1], d)
         pre = ["-include", os.path.join(d, "gen_params.h")]
-    inc = ["-I", SRC, "-I", os.path.join(HERE, "shim")]
+    src_dir = os.path.join(root, "src")
+    inc = ["-I", src_dir, "-I", os.path.join(HERE, "shim")]
     objs = []
     for unit in UNITS + ["GLUE"]:
-        src = os.path.join(HERE, "ref_glue.c") if unit == "GLUE" else os.path.join(SRC, unit)
+        src = os.path.join(HERE, "ref_glue.c") if unit == "GLUE" else os.path.join(src_dir, unit)
         obj = os.path.join(d, os.path.basename(src) + ".o")
         extra = list(pre)
         if dims is not None and unit == "ntt.c":
@@ -114,14 +124,71 @@ def build_variant(name, dims, force=False):
     return lib
 
 
-def build_all(force=False):
-    if not os.path.isdir(SRC):
+# --------------------------------------------------------------- GPU counter mapping (mode B)
+MODEB_FUNCS = ["__global__ void gaussian_sampler_S1_gpu(", "__global__ void gaussian_sampler_S2_gpu(",
+               "__device__ uint32_t add_mod_ntt_gpu_2(", "__global__ void gaussian_sampler_S3_gpu("]
+MODEB_FLAGS = ["-O2", "-fPIC", "-shared", "-std=c++17", "-w", "-fwrapv", "-fno-strict-aliasing",
+               "-ffp-contract=fast", "-march=x86-64-v3", "-ftrivial-auto-var-init=zero"]
+
+
+def extract_functions(text, heads):
+    """the text of each function definition starting with one of `heads`, unmodified, in file
+    order (from its head to the matching closing brace)"""
+    out = []
+    for head in heads:
+        i = text.index(head)
+        j = text.index("{", i)
+        depth = 0
+        for k in range(j, len(text)):
+            if text[k] == "{":
+                depth += 1
+            elif text[k] == "}":
+                depth -= 1
+                if depth == 0:
+                    out.append((i, text[i:k + 1]))
+                    break
+        else:
+            raise ValueError("unbalanced braces after " + head)
+    return [t for _, t in sorted(out)]
+
+
+def build_modeb(root, force=False):
+    """oracle/_ref/modeb/libmodeb.so: the reference's GPU sampler kernels (src/sample_gpu.cu) and
+    device headers compiled as host C++ by oracle/ref/modeb/modeb_host.cpp"""
+    d = os.path.join(OUT, "modeb")
+    lib = os.path.join(d, "libmodeb.so")
+    if os.path.exists(lib) and not force:
+        return lib
+    os.makedirs(d, exist_ok=True)
+    src_dir = os.path.join(root, "src")
+    with open(os.path.join(src_dir, "sample_gpu.cu")) as f:
+        text = f.read()
+    with open(os.path.join(d, "sample_gpu_kernels.inc"), "w") as f:
+        f.write("/* extracted from the reference's src/sample_gpu.cu by oracle/ref/build_ref.py; "
+                "not committed */\n")
+        for body in extract_functions(text, MODEB_FUNCS):
+            f.write(body + "\n\n")
+    shim = os.path.join(HERE, "modeb")
+    cmd = (["g++"] + MODEB_FLAGS + ["-I", shim, "-I", src_dir, "-I", d, "-o", lib,
+                                    os.path.join(shim, "modeb_host.cpp")])
+    subprocess.run(cmd, check=True)
+    return lib
+
+
+def build_all(root=None, force=False):
+    root = ref_root(root)
+    if not os.path.isdir(os.path.join(root, "src")):
         return False
     for name, dims in VARIANTS.items():
-        build_variant(name, dims, force)
+        build_variant(root, name, dims, force)
+    build_modeb(root, force)
     return True
 
 
 if __name__ == "__main__":
-    ok = build_all(force="--force" in sys.argv)
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--root", help="the reference tree (default: $CUFE_REFERENCE_ROOT)")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    ok = build_all(a.root, force=a.force)
     print("built" if ok else "reference sources absent; nothing built")

@@ -216,6 +216,31 @@ def test_c2_shape_golden_hashes():
     assert sha(cf.u32(dy)[0, 0]) == doc["dy"]
     d = cf.u32(dec)
     assert sha(d[0]) == doc["dec"] and int(d[0][0]) == doc["ip"]
+    # the same encryption with f_i drawn from the sigma_3 stream keyed by seed3 (as in the bench)
+    ct3 = c.encrypt(dev(x[None]), mpk, seed2[None], np.array(doc["seed3"], np.uint8)[None])
+    c.sync()
+    assert sha(cf.u32(ct3)[0]) == doc["ct_keyed"]
+    c.close()
+
+
+def test_sampler_gpu_map_golden():
+    """k_gauss_gpu_map against the reference's own GPU sampler kernels run on the host
+    (tests/golden/ref_modeb.npz): polynomial 0 in full, polynomials 1, 7, 63 by hash, every
+    sigma, two keys"""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_modeb.npz"))
+    hashes = json.loads(str(g["hashes"]))
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    q = np.array([16760833, 2147352577, 2130706433], np.int64)
+    c = cf.Context(4096, 4)
+    for k in range(2):
+        for sig in range(3):
+            got = cf.u32(c.sample_gpu_map(sig, g["keys"][k], 0, 64))
+            c.sync()
+            v = g["poly0_k%d_s%d" % (k, sig)].astype(np.int64)
+            want = np.stack([(v % qq).astype(np.uint32) for qq in q])
+            assert (canon(got[0]) == want).all(), (k, sig)
+            for bid in (1, 7, 63):
+                assert sha(canon(got[bid])) == hashes["k%d_s%d_b%d" % (k, sig, bid)], (k, sig, bid)
     c.close()
 
 

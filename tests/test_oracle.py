@@ -94,6 +94,55 @@ def test_c2_shape_hashes(oracle_built):
     assert sha(canon(sky)) == doc["sky"] and sha(canon(dy)) == doc["dy"]
     dec = O.decode(dy)
     assert sha(dec) == doc["dec"] and int(dec[0]) == doc["ip"] == doc["ip_plain"]
+    # f_i drawn from the sigma_3 stream keyed by seed3 (the bench's encryptions)
+    ct3 = O.encrypt(x, mpk, seed2, np.array(doc["seed3"], np.uint8))
+    assert sha(canon(ct3)) == doc["ct_keyed"]
+
+
+def _modeb_gold():
+    d = np.load(os.path.join(GOLD, "ref_modeb.npz"))
+    return {k: d[k] for k in d.files}
+
+
+def residues(v):
+    """canonical residues [3][n] of signed integers v"""
+    return np.stack([(v.astype(np.int64) % q).astype(np.uint32) for q in Q])
+
+
+def test_modeb_golden(oracle_built):
+    """the oracle's GPU counter mapping (mode B) against the reference's own GPU sampler kernels
+    run on the host (tests/golden/ref_modeb.npz): polynomial 0 of every sigma for two keys in
+    full, polynomials 1, 7 and 63 by hash"""
+    g = _modeb_gold()
+    hashes = json.loads(str(g["hashes"]))
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    O = Oracle(4096, 4)
+    for k in range(2):
+        rk = aes256_expand(g["keys"][k])
+        for sig in range(3):
+            assert (canon(O.gauss_modeB(rk, sig, 0)) == residues(g["poly0_k%d_s%d" % (k, sig)])).all(), (k, sig)
+            for bid in (1, 7, 63):
+                assert sha(canon(O.gauss_modeB(rk, sig, bid))) == hashes["k%d_s%d_b%d" % (k, sig, bid)], (k, sig, bid)
+
+
+def _have_modeb():
+    return os.path.exists(os.path.join(os.path.dirname(GOLD), "..", "oracle", "_ref", "modeb", "libmodeb.so"))
+
+
+@pytest.mark.skipif(not _have_modeb(), reason="host build of the reference GPU sampler not present")
+def test_modeb_random_keys_against_reference_kernels(oracle_built):
+    """fresh keys and polynomial indices: the oracle's mode B equals the reference's kernels
+    (src/sample_gpu.cu) run on the host, and its key schedule equals AESPrepareKey"""
+    from oracle.ffi import ReferenceModeB
+    M = ReferenceModeB()
+    O = Oracle(4096, 4)
+    rng = np.random.default_rng(0xC0FE0201)
+    for trial in range(3):
+        key = rng.integers(0, 256, 32, dtype=np.uint8)
+        rk = aes256_expand(key)
+        for sig in range(3):
+            bid = int(rng.integers(0, 64))
+            assert (canon(M.poly(sig, key, bid)) == canon(O.gauss_modeB(rk, sig, bid))).all(), (trial, sig, bid)
 
 
 def test_parameters(oracle_built):
