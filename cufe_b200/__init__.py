@@ -99,6 +99,7 @@ def lib():
             "cufe_server_read": [vp, ll, vp, C.c_size_t],
             "cufe_server_release": [vp, ll],
             "cufe_server_stats": [vp, vp, vp, vp],
+            "cufe_server_limits": [vp, i, C.c_double],
             "cufe_ring_set_variant": [vp, i, i],
             "cufe_ring_get_variant": [vp, vp, vp],
             "cufe_sampler_refills": [i, i, i],
@@ -122,6 +123,8 @@ def lib():
         L.cufe_profile_launches.restype = C.c_longlong
         for name in ("cufe_server_encrypt", "cufe_server_keygen", "cufe_server_decrypt"):
             getattr(L, name).restype = C.c_longlong
+        L.cufe_server_shed.argtypes = [vp]
+        L.cufe_server_shed.restype = C.c_longlong
         L.cufe_server_now.argtypes = []
         L.cufe_server_now.restype = C.c_double
         _lib = L
@@ -307,9 +310,16 @@ class Context:
         return dy
 
     def decrypt_noalloc(self, ct, y, sky, y_signed=False, dy=None, stream=None):
-        """decryption of one ciphertext with up to 4 keys, no device allocation in the call"""
+        """Decryption of one ciphertext ct[1][l+1][3][n] with up to 4 keys; the library call
+        allocates no device memory.  When dy is None this wrapper allocates the output with
+        torch, so a caller on a fixed device-memory budget passes its own dy[1][nkeys][3][n]."""
         nkeys = y.shape[0]
-        dy = _dev((1, nkeys, 3, self.n), self.dev) if dy is None else dy
+        if ct.shape[0] != 1:
+            raise ValueError("decrypt_noalloc takes exactly one ciphertext, got %d" % ct.shape[0])
+        if dy is None:
+            dy = _dev((1, nkeys, 3, self.n), self.dev)
+        elif tuple(dy.shape) != (1, nkeys, 3, self.n):
+            raise ValueError("dy must have shape (1, %d, 3, %d), got %s" % (nkeys, self.n, tuple(dy.shape)))
         _check(lib().cufe_decrypt_noalloc(self.h, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(dy),
                                           _stream(stream, self.device)), "cufe_decrypt_noalloc")
         return dy
@@ -517,7 +527,7 @@ class Server:
     """Request server over resident tenants (continuous batching): submit encrypt / keygen /
     decrypt requests, poll() to make progress, read results by request id."""
 
-    QUEUED, RUNNING, DONE, RELEASED = 0, 1, 2, 3
+    QUEUED, RUNNING, DONE, RELEASED, SHED = 0, 1, 2, 3, 4
 
     def __init__(self, n, l, arena_bytes=0, tick_bytes=0, device=0):
         self.n = np.ascontiguousarray(n, np.int32)
@@ -600,7 +610,16 @@ class Server:
     def stats(self):
         t, d, f = C.c_longlong(0), C.c_longlong(0), C.c_size_t(0)
         _check(lib().cufe_server_stats(self.h, C.byref(t), C.byref(d), C.byref(f)), "cufe_server_stats")
-        return {"ticks": t.value, "done": d.value, "ct_free_bytes": f.value}
+        shed = lib().cufe_server_shed(self.h)
+        if shed < 0:
+            raise CufeError(int(shed), "cufe_server_shed")
+        return {"ticks": t.value, "done": d.value, "ct_free_bytes": f.value, "shed": int(shed)}
+
+    def limits(self, max_tick_requests=0, max_queue_s=0.0):
+        """Overload control: at most max_tick_requests per tick (0: memory limits only); requests
+        queued longer than max_queue_s when a tick is formed are shed (0: never)."""
+        _check(lib().cufe_server_limits(self.h, int(max_tick_requests), float(max_queue_s)),
+               "cufe_server_limits")
 
 
 class SvmModel:

@@ -632,7 +632,7 @@ class WordArena {  // first-fit allocator over [0, words)
 };
 
 enum { REQ_ENCRYPT = 0, REQ_KEYGEN = 1, REQ_DECRYPT = 2 };
-enum { ST_QUEUED = 0, ST_RUNNING = 1, ST_DONE = 2, ST_RELEASED = 3 };
+enum { ST_QUEUED = 0, ST_RUNNING = 1, ST_DONE = 2, ST_RELEASED = 3, ST_SHED = 4 };
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -671,15 +671,20 @@ struct Server {
   size_t tab_bytes = 0, scr_bytes = 0;
   static constexpr int kMaxDec = 65536;
   static constexpr size_t kStageY = (size_t)32 << 20;  // pinned room for a tick's keygen vectors
-  uint64_t n_ticks = 0, n_done = 0;
+  uint64_t n_ticks = 0, n_done = 0, n_shed = 0;
+  // overload control: requests per tick (0: memory limits only) and the longest a request may
+  // wait in the queue before a tick admits it (0: forever); older requests are shed
+  int max_tick_reqs = 0;
+  double max_queue_s = 0;
 
   int create(int count, const int *n, const int *l, size_t arena_bytes, size_t tick_bytes, int dev) {
     device = dev;
     tenants.keys_only = true;  // the tenants' key pairs; ticks use the server's own scratch
     int rc = tenants.create(count, n, l, (size_t)1 << 40, dev);
     if (rc) return rc;
-    if (!arena_bytes) arena_bytes = (size_t)16 << 30;
-    if (!tick_bytes) tick_bytes = (size_t)16 << 30;
+    if ((rc = validate(count, n, l, arena_bytes, tick_bytes))) return rc;
+    if (!arena_bytes) arena_bytes = kDefaultBytes;
+    if (!tick_bytes) tick_bytes = kDefaultBytes;
     tab_bytes = (size_t)64 << 20;
     scr_bytes = tick_bytes;
     CUFE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -729,6 +734,37 @@ struct Server {
     return id;
   }
 
+  // tick scratch available to encryptions: 1 MiB stays for alignment and the key schedules
+  static uint64_t scratch_cap(uint64_t tick_bytes) { return tick_bytes > (1u << 20) ? tick_bytes - (1u << 20) : 0; }
+  uint64_t scratch_cap() const { return scratch_cap(scr_bytes); }
+
+  static constexpr size_t kDefaultBytes = (size_t)16 << 30;
+
+  // Tenant sizes, and every request of every tenant fitting an empty tick and an empty arena
+  // (a request that never fits would wait in the queue forever and block those behind it).
+  // Host-only: runs before any device is touched.
+  static int validate(int count, const int *n, const int *l, size_t arena_bytes, size_t tick_bytes) {
+    if (count < 1 || !n || !l) return CUFE_ERR_INVALID;
+    if (!arena_bytes) arena_bytes = kDefaultBytes;
+    if (!tick_bytes) tick_bytes = kDefaultBytes;
+    for (int t = 0; t < count; ++t) {
+      if (n[t] < 256 || n[t] > 8192 || (n[t] & (n[t] - 1)) || l[t] < 1 || l[t] > 4096) {
+        set_last_error("server: n must be a power of two in [256, 8192] and l in [1, 4096]");
+        return CUFE_ERR_INVALID;
+      }
+      const uint64_t need = enc_scratch_bytes((uint32_t)n[t], (uint32_t)l[t]);
+      const uint64_t ct_words = (uint64_t)(l[t] + 1) * 3 * n[t], sk_words = (uint64_t)3 * n[t] + l[t];
+      if (need > scratch_cap(tick_bytes) || ct_words > arena_bytes / 4 || sk_words > arena_bytes / 16) {
+        set_last_error("server: tenant " + std::to_string(t) + " (n=" + std::to_string(n[t]) +
+                       ", l=" + std::to_string(l[t]) + ") needs " + std::to_string(need + (1u << 20)) +
+                       " B of tick scratch and " + std::to_string(ct_words * 4) +
+                       " B of ciphertext arena; tick_bytes or arena_bytes is too small");
+        return CUFE_ERR_INVALID;
+      }
+    }
+    return CUFE_OK;
+  }
+
   static uint64_t enc_scratch_bytes(uint32_t n, uint32_t l) {
     const uint64_t poly = (uint64_t)3 * n * 4;
     const uint64_t R3 = cpu_map_refills(l, n, 2), R2 = cpu_map_refills(2, n, 1);
@@ -755,6 +791,19 @@ struct Server {
     t.ids.clear();
     t.dec_ids.clear();
     t.busy = false;
+  }
+
+  // drop a queued request without running it; a decrypt gives back its references
+  void shed(Req &r, double now) {
+    r.state = ST_SHED;
+    r.t_done = now;
+    ++n_shed;
+    if (r.kind == REQ_DECRYPT) {
+      for (int64_t ref : {r.ref_ct, r.ref_sk}) {
+        Req &o = reqs[ref];
+        if (--o.refs == 0 && o.release_pending) free_slot(o);
+      }
+    }
   }
 
   void free_slot(Req &o) {
@@ -793,11 +842,18 @@ struct Server {
     std::vector<int64_t> enc, kg, dec;
     uint64_t scr = 0, x_words = 0, blob_est = 1 << 16, ystage = 0;
     std::deque<int64_t> keep;
-    const uint64_t scr_cap = scr_bytes - (1u << 20);
+    const uint64_t scr_cap = scratch_cap();
+    const double now = now_s();
     while (!queue.empty()) {
+      if (max_tick_reqs > 0 && enc.size() + kg.size() + dec.size() >= (size_t)max_tick_reqs) break;
       const int64_t id = queue.front();
       queue.pop_front();
       Req &r = reqs[id];
+      if ((max_queue_s > 0 && now - r.t_arrival > max_queue_s) ||
+          (r.kind == REQ_DECRYPT && (reqs[r.ref_ct].state == ST_SHED || reqs[r.ref_sk].state == ST_SHED))) {
+        shed(r, now);
+        continue;
+      }
       const InstDev &I = tenant(r.tenant);
       bool ok = true;
       if (r.kind == REQ_ENCRYPT) {
@@ -1177,6 +1233,7 @@ int cufe_server_create(cufe_server **out, int tenants, const int *n, const int *
                        size_t tick_bytes, int device) {
   if (!out) return CUFE_ERR_INVALID;
   *out = nullptr;
+  if (int rc = cufe::Server::validate(tenants, n, l, arena_bytes, tick_bytes)) return rc;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cufe::set_last_error("no CUDA device");
@@ -1244,7 +1301,8 @@ long long cufe_server_decrypt(cufe_server *h, long long ct, long long sk, double
   auto &R = h->s.reqs;
   if (ct < 0 || sk < 0 || ct >= (long long)R.size() || sk >= (long long)R.size() ||
       R[ct].kind != cufe::REQ_ENCRYPT || R[sk].kind != cufe::REQ_KEYGEN || R[ct].tenant != R[sk].tenant ||
-      R[ct].state == cufe::ST_RELEASED || R[sk].state == cufe::ST_RELEASED || R[ct].release_pending ||
+      R[ct].state == cufe::ST_RELEASED || R[sk].state == cufe::ST_RELEASED || R[ct].state == cufe::ST_SHED ||
+      R[sk].state == cufe::ST_SHED || R[ct].release_pending ||
       R[sk].release_pending) {
     cufe::set_last_error("decrypt: needs a live ciphertext and function key of the same tenant");
     return CUFE_ERR_INVALID;
@@ -1306,6 +1364,20 @@ int cufe_server_release(cufe_server *h, long long id) {
   r.release_pending = true;
   if (r.refs == 0) h->s.free_slot(r);
   return CUFE_OK;
+}
+
+int cufe_server_limits(cufe_server *h, int max_tick_requests, double max_queue_seconds) {
+  if (!h || max_tick_requests < 0 || !(max_queue_seconds >= 0)) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  h->s.max_tick_reqs = max_tick_requests;
+  h->s.max_queue_s = max_queue_seconds;
+  return CUFE_OK;
+}
+
+long long cufe_server_shed(cufe_server *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  return (long long)h->s.n_shed;
 }
 
 int cufe_server_stats(cufe_server *h, long long *ticks, long long *done, size_t *ct_free_bytes) {

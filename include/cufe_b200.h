@@ -291,7 +291,8 @@ long long cufe_server_decrypt(cufe_server *server, long long ciphertext, long lo
  * flight.  Returns the number of requests completed by this call or a negative status. */
 int cufe_server_poll(cufe_server *server, int wait);
 int cufe_server_pending(cufe_server *server, long long *queued, int *ticks_in_flight);
-/* state: 0 queued, 1 running, 2 done, 3 released; value: a decrypt's result */
+/* state: 0 queued, 1 running, 2 done, 3 released, 4 shed (dropped unrun by the overload
+ * limits below; no result); value: a decrypt's result */
 int cufe_server_result(cufe_server *server, long long id, int *state, uint32_t *value, double *t_arrival,
                        double *t_done);
 /* copy a finished encrypt's ciphertext [(l+1)][3][n] or keygen's function key [3][n] (then
@@ -300,6 +301,15 @@ int cufe_server_read(cufe_server *server, long long id, uint32_t *host, size_t w
 /* free a finished encrypt's or keygen's slot once no queued decrypt reads it */
 int cufe_server_release(cufe_server *server, long long id);
 int cufe_server_stats(cufe_server *server, long long *ticks, long long *done, size_t *ct_free_bytes);
+/* Overload control.  A tick admits at most max_tick_requests requests (0: only the memory
+ * limits), which bounds how long one tick runs; a queued request that has waited longer than
+ * max_queue_seconds (0: no limit) when a tick is formed is shed instead of run (state 4), and so
+ * is a decrypt that reads a shed encrypt or keygen.  A completed request's latency is then at
+ * most max_queue_seconds plus the time of the tick before it and its own.  Applies from the next
+ * tick on. */
+int cufe_server_limits(cufe_server *server, int max_tick_requests, double max_queue_seconds);
+/* requests shed so far (or a negative status) */
+long long cufe_server_shed(cufe_server *server);
 
 /* =====================================================================================
  * 3. Negacyclic NTT on an RNS ring (CT_forward / GS_reverse, src/ntt.c:38-114)

@@ -79,6 +79,29 @@ def test_argument_checks_before_device_use():
     assert L.cufe_dropin_status() == -1
 
 
+def test_server_refuses_sizes_that_never_fit():
+    """a tenant whose single encryption does not fit an empty tick (or whose ciphertext does not
+    fit the arena) is refused at create, before any device is touched; so is a tick_bytes below
+    the 1 MiB the server keeps for itself"""
+    import ctypes as C
+    import cufe_b200 as cf
+    L = cf.lib()
+    h = C.c_void_p()
+    n = np.array([4096], np.int32)
+    l = np.array([784], np.int32)
+
+    def create(arena, tick, nn=n, ll=l):
+        return L.cufe_server_create(C.byref(h), len(nn), nn.ctypes.data, ll.ctypes.data, arena, tick, 0)
+
+    assert create(0, 1 << 19) == -1                     # below the server's own 1 MiB
+    assert b"tick_bytes or arena_bytes is too small" in L.cufe_last_error()
+    assert create(0, 64 << 20) == -1                    # one l = 784 encryption needs ~140 MB
+    assert create(32 << 20, 0) == -1                    # a 38.6 MB ciphertext in a 32 MiB arena
+    assert create(0, 0, np.array([4096, 3000], np.int32), np.array([8, 8], np.int32)) == -1
+    if _no_gpu():                                       # sizes that fit reach the device check
+        assert create(0, 1 << 30) == -5 and create(64 << 20, 256 << 20, ll=np.array([16], np.int32)) == -5
+
+
 def test_sampler_refill_sizing():
     import cufe_b200 as cf
     L = cf.lib()
