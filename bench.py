@@ -487,6 +487,25 @@ def gpu_arm(args):
             "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "clocks": clocks}
+    # the other configurations, compact, on the same box (one GPU only): the C2 buffers go first
+    if world == 1 and not args.no_extras:
+        del ct, dy, res, scratch, r0, pl_ct, pl_dy, pl_out, xd, x_dev, y_dev, sky, mpk, msk
+        ctx.close()
+        torch.cuda.empty_cache()
+        line["c4_ntt"] = ntt_point(4096, 3, 65536, 10, 3)
+        mixed = mixed_measure(4096, 5, 3, 24)
+        line["c3_batched"] = {k: mixed[k] for k in ("value", "unit", "ms_per_step", "p50_ms", "p99_ms", "bit_exact",
+                                                    "setup_s", "graph", "sigma3_samples_per_s")}
+        line["c3_batched"]["config"] = mixed["config"]
+        serve = serve_measure(64, [5000, 10000, 20000, 50000], 0.5, 48, 24, 30,
+                              max_tick=args.serve_max_tick, max_queue_s=args.serve_max_queue_ms / 1000.0)
+        line["c5_serving"] = {"config": serve["config"], "plain": serve["plain"], "bit_exact": serve["bit_exact"],
+                              "results": [{k: r[k] for k in ("rate_rps", "submitted", "completed", "shed",
+                                                             "goodput_rps", "bit_exact", "ticks")} |
+                                          {"p50_ms": (r["latency"]["all"] or {}).get("p50_ms"),
+                                           "p99_ms": (r["latency"]["all"] or {}).get("p99_ms")}
+                                          for r in serve["results"]]}
+        bit_exact = bit_exact and line["c4_ntt"]["roundtrip_ok"] and mixed["bit_exact"] and serve["bit_exact"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline_sample(x, y, seeds2, setup_seeds,
@@ -495,7 +514,8 @@ def gpu_arm(args):
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
+    if world > 1 or args.no_extras:
+        ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0 if bit_exact else 1
@@ -584,6 +604,53 @@ def ntt_sweep(args):
     return 0 if line["all_roundtrips_ok"] else 1
 
 
+def ntt_point(n, k, npoly, steps, warmup):
+    """one point of the kernel sweep with the tuner's variant: forward and inverse negacyclic NTT
+    over npoly polynomials of k residues (uniform in [0, q_j), seed 0xC0FE0004), median of
+    `steps` event-timed passes, 8n bytes per residue polynomial per pass; the data must come
+    back unchanged after every forward + inverse"""
+    import torch
+    import cufe_b200 as cf
+    dev = "cuda:0"
+    peak = _peaks().get("hbm_gbs", 6650.0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0xC0FE0004)
+    ring = cf.Ring(n, k)
+    data = torch.empty((npoly, k, n), dtype=torch.int32, device=dev)
+    for j in range(k):
+        data[:, j, :] = torch.randint(0, int(ring.primes[j]), (npoly, n), generator=g, device=dev,
+                                      dtype=torch.int64).to(torch.int32)
+    orig = data.clone()
+    tuned = ring.tune(npoly)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        ring.forward(data)
+        ring.inverse(data)
+    fwd, inv = [], []
+    for _ in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        ring.forward(data)
+        ev[1].record(stream)
+        ring.inverse(data)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        fwd.append(ev[0].elapsed_time(ev[1]))
+        inv.append(ev[1].elapsed_time(ev[2]))
+    ok = bool(torch.equal(data, orig))
+    nbytes = 8 * n * npoly * k
+    f_ms, i_ms = float(np.median(fwd)), float(np.median(inv))
+    out = {"n": n, "k": k, "polys": npoly, "bytes_per_pass": nbytes, "fwd_ms": f_ms, "inv_ms": i_ms,
+           "fwd_gbs": nbytes / f_ms / 1e6, "inv_gbs": nbytes / i_ms / 1e6,
+           "fwd_frac": nbytes / f_ms / 1e6 / peak, "inv_frac": nbytes / i_ms / 1e6 / peak,
+           "peak_gbs": peak, "peak_source": "measured" if "hbm_gbs" in _peaks() else "fallback",
+           "tuned_variant": list(tuned["variant"]), "roundtrip_ok": ok}
+    del data, orig
+    ring.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def sampler_sweep(args):
     """2^30 discrete Gaussian samples per sigma in both mappings at n = 4096: samples/s over
     the sampler launches (CUDA events) and Pearson chi-square on 1000 equiprobable bins of
@@ -655,16 +722,25 @@ def splitmix64(x):
 
 
 def batched_mixed(args):
-    """Heterogeneous batch: 4,096 independent IPFE instances, l = round(exp(U[ln 32, ln 1024])),
+    """the heterogeneous batch as its own workload line (see mixed_measure)"""
+    import torch
+    torch.cuda.set_device(0)
+    line = mixed_measure(args.instances, args.steps, args.warmup, args.chunk_gb)
+    print(json.dumps(line), flush=True)
+    return 0 if line["bit_exact"] else 1
+
+
+def mixed_measure(count, steps, warmup, chunk_gb):
+    """Heterogeneous batch: `count` independent IPFE instances, l = round(exp(U[ln 32, ln 1024])),
     N in {2048, 4096} 50/50, x in [0, 4], y in [-16, 16]; instance i's data from
     SplitMix64(0xC0FE0003 + i).  Keys are generated once (setup timed separately) and stay
     resident; a step is one replay of the batch's CUDA graph (encrypt + keygen + decrypt +
     decode of every instance) with fresh encryption seeds copied in from pinned host memory.
-    Every inner product of the timed steps is checked against the plaintext dot product."""
+    Every inner product of the timed steps is checked against the plaintext dot product.
+    Launch gaps: one more step runs eagerly with CUDA events around every kernel group;
+    replay time / summed kernel time is the graph's cost over its kernels."""
     import torch
     import cufe_b200 as cf
-    torch.cuda.set_device(0)
-    count = args.instances
     ns, ls, xs, ys, seeds = [], [], [], [], []
     for i in range(count):
         r = np.random.default_rng(splitmix64(0xC0FE0003 + i))
@@ -675,80 +751,109 @@ def batched_mixed(args):
         seeds.append(r.integers(0, 256, (3, 32), dtype=np.uint8))
     seeds = np.stack(seeds)
     t0 = time.perf_counter()
-    B = cf.Batch(ns, ls, max_chunk_bytes=args.chunk_gb << 30)
+    B = cf.Batch(ns, ls, max_chunk_bytes=chunk_gb << 30)
     B.setup(seeds[:, 0], seeds[:, 1], seeds[:, 2])
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     x = cf.to_dev(B.pack(xs).astype(np.uint32))
     y = cf.to_dev(B.pack(ys).astype(np.int32))
     rng = np.random.default_rng(0xC0FE0003)
-    total = args.warmup + args.steps
+    total = warmup + steps + 1
     host_seeds = torch.from_numpy(rng.integers(0, 256, (total, 2, count, 32), dtype=np.uint8)).pin_memory()
     s2 = torch.empty((count, 32), dtype=torch.uint8, device="cuda:0")
     s3 = torch.empty_like(s2)
     out = B.bind(x, y, s2, s3)
-    res = torch.empty((args.steps, count), dtype=torch.int32, device="cuda:0")
+    res = torch.empty((steps + 1, count), dtype=torch.int32, device="cuda:0")
     stream = torch.cuda.current_stream()
 
-    def step(k):
+    def seeds_in(k):
         s2.copy_(host_seeds[k, 0], non_blocking=True)
         s3.copy_(host_seeds[k, 1], non_blocking=True)
-        B.replay()
 
-    for k in range(args.warmup):
-        step(k)
+    for k in range(warmup):
+        seeds_in(k)
+        B.replay()
     torch.cuda.synchronize()
     B.status()
     clk = Clocks(0, os.path.join(tempfile.gettempdir(), "cufe_clocks_mixed.csv"))
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     ev[0].record(stream)
-    for k in range(args.steps):
-        step(args.warmup + k)
+    for k in range(steps):
+        seeds_in(warmup + k)
+        B.replay()
         res[k].copy_(out)
         ev[k + 1].record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
     B.status()
-    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    ms = ev[0].elapsed_time(ev[args.steps])
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+    ms = ev[0].elapsed_time(ev[steps])
+    # one eager step with kernel timing: the replay's launch gaps against its kernel time
+    seeds_in(warmup + steps)
+    torch.cuda.synchronize()
+    B.profile(True)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    B.run()
+    g1.record(stream)
+    res[steps].copy_(out)
+    torch.cuda.synchronize()
+    kernel_ms, kernels = B.profile_read()
+    B.profile(False)
+    eager_ms = g0.elapsed_time(g1)
     p = np.array([64 * l + 1 for l in ls], np.int64)
     exp = np.array([int(a @ b) for a, b in zip(xs, ys)], np.int64) % p
     got = cf.u32(res).astype(np.int64) % p[None, :]
     ok = bool((got == exp[None, :]).all())
     samples = sum(l * n for l, n in zip(ls, ns))
+    replay_ms = float(np.median(step_ms))
     line = {"workload": "batched-mixed", "metric": "IPFE inner products/sec, heterogeneous batch (bit-exact)",
-            "value": args.steps * count / (ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "p50_ms": float(np.percentile(step_ms, 50)),
+            "value": steps * count / (ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms / steps, "p50_ms": float(np.percentile(step_ms, 50)),
             "p99_ms": float(np.percentile(step_ms, 99)), "higher_is_better": True, "dtype": "uint32",
             "data": "synthetic", "bit_exact": ok, "setup_s": setup_s,
+            "graph": {"kernels": B.graph_kernels(), "replay_ms": replay_ms,
+                      "eager_kernel_ms": kernel_ms, "eager_kernels": kernels, "eager_step_ms": eager_ms,
+                      "replay_over_kernel_time": replay_ms / kernel_ms if kernel_ms else None,
+                      "note": "kernel time from CUDA events around every kernel group of one eager step"},
             "config": {"workload": "%d instances, l log-uniform [32, 1024], N 2048/4096 50/50, one CUDA graph "
                                    "replay per step" % count,
                        "instances": count, "mean_l": float(np.mean(ls)), "n4096_share": float(np.mean(np.array(ns) == 4096)),
                        "chunks": B.chunks, "key_gb": B.key_bytes / 1e9, "scratch_gb": B.scratch_bytes / 1e9,
                        "sigma3_samples_per_step": samples},
-            "sigma3_samples_per_s": samples / (ms / args.steps / 1000.0), "clocks": clocks}
-    print(json.dumps(line), flush=True)
+            "sigma3_samples_per_s": samples / (ms / steps / 1000.0), "clocks": clocks}
     B.close()
-    return 0 if ok else 1
+    return line
 
 
 def serving(args):
+    """the serving loop as its own workload line (see serve_measure)"""
+    import torch
+    torch.cuda.set_device(0)
+    line = serve_measure(args.tenants, args.rates, args.duration, args.arena_gb, args.tick_gb,
+                         args.plain_requests, args.max_tick, args.max_queue_ms / 1000.0)
+    print(json.dumps(line), flush=True)
+    return 0 if line["bit_exact"] else 1
+
+
+def serve_measure(T, rates, duration, arena_gb, tick_gb, plain_requests, max_tick=0, max_queue_s=0.0):
     """Serving loop: open-loop Poisson arrivals at each rate for `duration` seconds, request mix
-    encrypt:keygen:decrypt = 4:1:4, tenants with l log-uniform in [64, 1024] and N in
+    encrypt:keygen:decrypt = 4:1:4, T tenants with l log-uniform in [64, 1024] and N in
     {2048, 4096} (keys resident), seeded from SplitMix64(0xC0FE0005 + i).  Decryptions read a
     resident pool of ciphertexts and function keys per tenant (their inner products are
     checked); new ciphertexts and keys are released as they complete.  Latency = completion
-    seen by the server's poll minus the scheduled arrival time.  The plain form serves a
-    sample of the same requests one per tick, each to completion, on the same kernels."""
+    seen by the server's poll minus the scheduled arrival time, over completed requests.
+    With overload limits (max_tick requests per tick, max_queue_s of queueing) requests that
+    waited too long are shed; goodput counts completed requests only.  The plain form serves
+    a sample of the same requests one per tick, each to completion, on the same kernels."""
     import cufe_b200 as cf
-    T = args.tenants
     ns, ls = [], []
     for i in range(T):
         r = np.random.default_rng(splitmix64(0xC0FE0005 + i))
         ls.append(int(round(float(np.exp(r.uniform(np.log(64), np.log(1024)))))))
         ns.append(2048 if r.random() < 0.5 else 4096)
     rng = np.random.default_rng(0xC0FE0005)
-    S = cf.Server(ns, ls, arena_bytes=args.arena_gb << 30, tick_bytes=args.tick_gb << 30)
+    S = cf.Server(ns, ls, arena_bytes=arena_gb << 30, tick_bytes=tick_gb << 30)
     S.setup(rng.integers(0, 256, (T, 32), dtype=np.uint8), None, rng.integers(0, 256, (T, 32), dtype=np.uint8))
     # resident pool: 2 ciphertexts and 2 function keys per tenant
     pool = []
@@ -760,6 +865,7 @@ def serving(args):
         sks = [S.keygen(t, y) for y in ys]
         pool.append((xs, ys, cts, sks))
     S.drain()
+    S.limits(max_tick, max_queue_s)
     kinds = np.array([0] * 4 + [1] + [2] * 4)
 
     def make_requests(k, rate):
@@ -787,17 +893,29 @@ def serving(args):
         return S.decrypt(cts[req[3]], sks[req[4]], t_arr)
 
     def check(req, rid):
+        """(finished state is valid and a decrypt's value is right, completed, latency ms)"""
         st, v, ta, td = S.result(rid)
+        if st == S.SHED:
+            return True, False, None
         ok = st in (S.DONE, S.RELEASED)
         if req[1] == 2:
             xs, ys, _, _ = pool[req[2]]
             p = 64 * ls[req[2]] + 1
             ok = ok and v % p == int(xs[req[3]].astype(np.int64) @ ys[req[4]].astype(np.int64)) % p
-        return ok, 1000.0 * (td - ta)
+        return ok, True, 1000.0 * (td - ta)
+
+    def release_finished(owned):
+        while owned:
+            st = S.result(owned[0])[0]
+            if st not in (S.DONE, S.SHED):
+                return
+            rid = owned.pop(0)
+            if st == S.DONE:
+                S.release(rid)
 
     results = []
-    for rate in args.rates:
-        reqs = make_requests(max(1, int(rate * args.duration)), rate)
+    for rate in rates:
+        reqs = make_requests(max(1, int(rate * duration)), rate)
         t0 = S.now() + 0.01
         ids, owned = [], []
         t_pos = 0
@@ -811,43 +929,46 @@ def serving(args):
                     owned.append(rid)
                 t_pos += 1
             S.poll()
-            # release finished ciphertexts / keys (oldest first) to bound the arenas
-            while owned and S.result(owned[0])[0] == S.DONE:
-                S.release(owned.pop(0))
+            release_finished(owned)  # bound the arenas
         while True:
             q, fl = S.pending()
-            while owned and S.result(owned[0])[0] == S.DONE:
-                S.release(owned.pop(0))
+            release_finished(owned)
             if q == 0 and fl == 0:
                 break
             S.poll(wait=fl > 0)
-        t_end = max(S.result(i)[3] for i in ids)
         lat = {0: [], 1: [], 2: []}
-        ok = True
+        ok, completed, t_end = True, 0, t0
         for req, rid in zip(reqs, ids):
-            good, ms = check(req, rid)
+            good, done, ms = check(req, rid)
             ok = ok and good
-            lat[req[1]].append(ms)
+            if done:
+                completed += 1
+                lat[req[1]].append(ms)
+                t_end = max(t_end, S.result(rid)[3])
         for rid in owned:
-            S.release(rid)
+            if S.result(rid)[0] == S.DONE:
+                S.release(rid)
         st = S.stats()
         allv = lat[0] + lat[1] + lat[2]
         pct = lambda v: {"p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99)),  # noqa: E731
                          "n": len(v)} if v else None
-        results.append({"rate_rps": rate, "submitted": len(reqs), "bit_exact": ok,
-                        "throughput_rps": len(reqs) / (t_end - t0), "span_s": t_end - t0,
+        span = max(t_end - t0, 1e-9)
+        results.append({"rate_rps": rate, "submitted": len(reqs), "completed": completed,
+                        "shed": st["shed"] - t_stat0["shed"], "bit_exact": ok,
+                        "goodput_rps": completed / span, "span_s": span,
                         "latency": {"all": pct(allv), "encrypt": pct(lat[0]), "keygen": pct(lat[1]),
                                     "decrypt": pct(lat[2])},
                         "ticks": st["ticks"] - t_stat0["ticks"],
-                        "requests_per_tick": len(reqs) / max(1, st["ticks"] - t_stat0["ticks"])})
+                        "requests_per_tick": completed / max(1, st["ticks"] - t_stat0["ticks"])})
+    S.limits(0, 0.0)
     # plain per-call form: one request per tick, run to completion, same kernels
-    sample = make_requests(args.plain_requests, 1000.0)
+    sample = make_requests(plain_requests, 1000.0)
     plat = []
     for req in sample:
         t_a = S.now()
         rid = submit(req, t_a)
         S.drain()
-        good, ms = check(req, rid)
+        good, _, ms = check(req, rid)
         plat.append(ms)
         if req[1] != 2:
             S.release(rid)
@@ -857,12 +978,12 @@ def serving(args):
     line = {"workload": "serving", "metric": "requests/s and p50/p99 latency, encrypt:keygen:decrypt = 4:1:4",
             "unit": "req/s", "n_gpus": 1, "data": "synthetic", "dtype": "uint32",
             "config": {"tenants": T, "mean_l": float(np.mean(ls)), "n4096_share": float(np.mean(np.array(ns) == 4096)),
-                       "duration_s": args.duration, "arena_gb": args.arena_gb, "tick_gb": args.tick_gb},
+                       "duration_s": duration, "arena_gb": arena_gb, "tick_gb": tick_gb,
+                       "max_tick_requests": max_tick, "max_queue_ms": 1000.0 * max_queue_s},
             "results": results, "plain": plain,
             "bit_exact": all(r["bit_exact"] for r in results)}
-    print(json.dumps(line), flush=True)
     S.close()
-    return 0 if line["bit_exact"] else 1
+    return line
 
 
 def _svm_ref_init(path):
@@ -1011,6 +1132,11 @@ def main():
     ap.add_argument("--arena-gb", type=int, default=48)
     ap.add_argument("--tick-gb", type=int, default=24)
     ap.add_argument("--plain-requests", type=int, default=100)
+    ap.add_argument("--max-tick", type=int, default=0, help="serving: requests per tick (0: memory only)")
+    ap.add_argument("--max-queue-ms", type=float, default=0.0, help="serving: shed requests queued longer")
+    ap.add_argument("--no-extras", action="store_true", help="pipeline: skip the C3/C4/C5 sub-measurements")
+    ap.add_argument("--serve-max-tick", type=int, default=512, help="pipeline's serving sub-line: per-tick cap")
+    ap.add_argument("--serve-max-queue-ms", type=float, default=50.0, help="pipeline's serving sub-line: deadline")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--chunk-gb", type=int, default=24)
     ap.add_argument("--sweep-polys", type=int, default=65536)

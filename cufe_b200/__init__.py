@@ -84,6 +84,9 @@ def lib():
             "cufe_batch_status": [vp],
             "cufe_batch_info": [vp, vp, vp, vp, vp],
             "cufe_batch_instance": [vp, i, vp, vp, vp, vp],
+            "cufe_batch_profile": [vp, i],
+            "cufe_batch_profile_read": [vp, vp, vp],
+            "cufe_batch_graph_kernels": [vp],
             "cufe_svm_create": [C.POINTER(vp), vp, i, i, vp, i, vp, vp, vp, vp, vp, vp],
             "cufe_svm_predict": [vp, i, vp, vp, vp, vp, vp],
             "cufe_svm_destroy": [vp],
@@ -501,6 +504,22 @@ class Batch:
 
     def replay(self, stream=None):
         _check(lib().cufe_batch_replay(self.h, _stream(stream, self.device)), "cufe_batch_replay")
+
+    def profile(self, on):
+        """kernel timing of eager steps (run()); on clears the totals"""
+        _check(lib().cufe_batch_profile(self.h, int(on)), "cufe_batch_profile")
+
+    def profile_read(self):
+        """(summed kernel milliseconds, kernels launched) of the profiled eager steps"""
+        ms, k = C.c_double(0), C.c_longlong(0)
+        _check(lib().cufe_batch_profile_read(self.h, C.byref(ms), C.byref(k)), "cufe_batch_profile_read")
+        return ms.value, k.value
+
+    def graph_kernels(self):
+        r = lib().cufe_batch_graph_kernels(self.h)
+        if r < 0:
+            raise CufeError(r, "cufe_batch_graph_kernels")
+        return r
 
     def status(self):
         _check(lib().cufe_batch_status(self.h), "cufe_batch_status")

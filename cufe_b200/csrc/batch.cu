@@ -1107,6 +1107,7 @@ struct Server {
 struct cufe_batch {
   cufe::Batch b;
   std::mutex mu;
+  cufe::Prof prof;  // eager steps' kernel timing (cufe_batch_profile)
 };
 
 extern "C" {
@@ -1167,7 +1168,52 @@ int cufe_batch_run(cufe_batch *h, void *stream) {
   if (!h) return CUFE_ERR_INVALID;
   std::lock_guard<std::mutex> g(h->mu);
   if (cudaSetDevice(h->b.device) != cudaSuccess) return CUFE_ERR_CUDA;
-  return h->b.run(static_cast<cudaStream_t>(stream));
+  cufe::t_prof = &h->prof;
+  const int rc = h->b.run(static_cast<cudaStream_t>(stream));
+  cufe::t_prof = nullptr;
+  return rc;
+}
+
+int cufe_batch_profile(cufe_batch *h, int on) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  h->prof.collect();
+  h->prof.acc.clear();
+  h->prof.kernels = 0;
+  h->prof.on = on != 0;
+  return CUFE_OK;
+}
+
+int cufe_batch_profile_read(cufe_batch *h, double *kernel_ms, long long *kernels) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  h->prof.collect();
+  double ms = 0;
+  long long k = 0;
+  for (const auto &kv : h->prof.acc) {
+    ms += kv.second.second;
+    k += kv.second.first;
+  }
+  if (kernel_ms) *kernel_ms = ms;
+  if (kernels) *kernels = k;
+  return CUFE_OK;
+}
+
+int cufe_batch_graph_kernels(cufe_batch *h) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->b.graph) return 0;
+  size_t nodes = 0;
+  if (cudaGraphGetNodes(h->b.graph, nullptr, &nodes) != cudaSuccess) return CUFE_ERR_CUDA;
+  std::vector<cudaGraphNode_t> v(nodes);
+  if (nodes && cudaGraphGetNodes(h->b.graph, v.data(), &nodes) != cudaSuccess) return CUFE_ERR_CUDA;
+  int kernels = 0;
+  for (cudaGraphNode_t nd : v) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) return CUFE_ERR_CUDA;
+    kernels += t == cudaGraphNodeTypeKernel;
+  }
+  return kernels;
 }
 
 int cufe_batch_replay(cufe_batch *h, void *stream) {

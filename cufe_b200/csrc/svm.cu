@@ -22,11 +22,25 @@ namespace {
 
 constexpr int kMaxClasses = 64;
 
-// One thread per test vector: the vote of main.c:331-379, in its order.  The reference's
-// host code is built with -O3 -march=native (Makefile), where gcc contracts
-// `sum += coef * kvalue` into a fused multiply-add; the sums here use fma in the same order.
-// kvalue is the decoded coefficient 0 in [0, p]; for signed support vectors it is centred
-// into (-p/2, p/2] (the reference only has unsigned y and uses the value as decoded).
+// One term loop of the vote, `for (k = 0; k < cnt; k++) sum += coef[k] * kvalue[k]`
+// (main.c:359-362), with the arithmetic gcc -O3 gives it on an AVX2 + FMA host (the
+// reference's Makefile builds with -O3 -march=native -mavx2): the loop is vectorised as an
+// in-order reduction, 4 products at a time (vmulpd: each product rounded) added to the sum one
+// after another (vaddsd), then a 2-wide epilogue the same way, and an odd last term in the
+// scalar remainder, where the multiply-add is contracted to one fused multiply-add.  So every
+// product is rounded before its addition except the last one of an odd-length loop.
+template <class F>
+__device__ double vote_terms(double sum, const double *__restrict__ coef, F value, int first, int cnt) {
+  const int paired = cnt & ~1;
+  for (int k = 0; k < paired; ++k) sum = __dadd_rn(sum, __dmul_rn(coef[first + k], value(first + k)));
+  if (cnt & 1) sum = __fma_rn(coef[first + paired], value(first + paired), sum);
+  return sum;
+}
+
+// One thread per test vector: the vote of main.c:331-379, in its order, the term loops as
+// vote_terms computes them.  kvalue is the decoded coefficient 0 in [0, p]; for signed support
+// vectors it is centred into (-p/2, p/2] (the reference only has unsigned y and uses the value
+// as decoded).
 __global__ void k_svm_vote(const uint32_t *__restrict__ kval, int nct, int lsv, uint32_t p, int centre,
                            int nr_class, const double *__restrict__ coef, const double *__restrict__ rho,
                            const int *__restrict__ nsv, const int *__restrict__ label, int *__restrict__ out,
@@ -53,8 +67,8 @@ __global__ void k_svm_vote(const uint32_t *__restrict__ kval, int nct, int lsv, 
       double sum = 0;
       const int si = start[i], sj = start[j], ci = nsv[i], cj = nsv[j];
       const double *coef1 = coef + (size_t)(j - 1) * lsv, *coef2 = coef + (size_t)i * lsv;
-      for (int k = 0; k < ci; ++k) sum = fma(coef1[si + k], value(si + k), sum);
-      for (int k = 0; k < cj; ++k) sum = fma(coef2[sj + k], value(sj + k), sum);
+      sum = vote_terms(sum, coef1, value, si, ci);
+      sum = vote_terms(sum, coef2, value, sj, cj);
       sum -= rho[pp];
       if (dec) dec[(size_t)t * npairs + pp] = sum;
       if (sum > 0)

@@ -247,6 +247,14 @@ int cufe_batch_run(cufe_batch *batch, void *stream);
  * that call if none ran) and replayed afterwards: the graph reads the bound buffers' current
  * contents, so new seeds or inputs written there take effect on the next replay */
 int cufe_batch_replay(cufe_batch *batch, void *stream);
+/* kernel timing of eager steps (cufe_batch_run): on != 0 clears and starts it; read gives the
+ * summed device milliseconds of the step's kernel groups (CUDA events around each group on the
+ * step's stream) and the number of kernels launched; with it the cost of the graph's launch
+ * gaps is replay time / kernel time.  No counterpart in the reference. */
+int cufe_batch_profile(cufe_batch *batch, int on);
+int cufe_batch_profile_read(cufe_batch *batch, double *kernel_ms, long long *kernels);
+/* kernel nodes of the captured step graph (0 before the first replay) */
+int cufe_batch_graph_kernels(cufe_batch *batch);
 /* synchronous check of the batch's sampler status word (CUFE_ERR_SAMPLER if set) */
 int cufe_batch_status(cufe_batch *batch);
 /* x_off[count + 1] (may be NULL), number of chunks, resident key bytes, scratch bytes */

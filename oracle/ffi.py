@@ -324,3 +324,72 @@ class ReferenceModeB:
         if rc:
             raise RuntimeError("modeb_block failed: %d" % rc)
         return out.reshape(3, self.n)
+
+
+class ReferenceCallers:
+    """The reference's own callers of the GPU entry points (main.c, src/rlwe_sife.c, svm.cpp;
+    n = 2048, l = 124) linked against cufe_b200/libcufe_b200.so: oracle/_ref/callers/."""
+
+    PATH = os.path.join(HERE, "_ref", "callers", "libcallers.so")
+
+    def __init__(self):
+        L = _load(self.PATH)
+        vp = C.c_void_p
+        L.cl_n.restype = C.c_int
+        L.cl_l.restype = C.c_int
+        L.cl_queue_seeds.argtypes = [_u8p, C.c_int]
+        L.cl_load_model.restype = vp
+        L.cl_load_model.argtypes = [C.c_char_p]
+        L.cl_free_model.argtypes = [vp]
+        L.cl_model_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.cl_model_arrays.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.cl_predict_plain.restype = C.c_double
+        L.cl_predict_plain.argtypes = [vp, _u32p]
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        for f in (L.cl_predict_cpu, L.cl_predict_gpu):
+            f.restype = C.c_double
+            f.argtypes = [vp, _u32p, _u32p, f64p, f64p]
+        L.cl_setup.argtypes = [_u32p, _u32p]
+        L.cl_encrypt.argtypes = [_u32p, _u32p, _u32p]
+        L.cl_setup_gui.argtypes = [_u32p, _u32p]
+        L.cl_encrypt_gui.argtypes = [_u32p, _u32p, _u32p, C.c_int]
+        self.L = L
+        self.n, self.l = L.cl_n(), L.cl_l()
+
+    def seeds(self, *seeds):
+        s = np.concatenate([np.ascontiguousarray(x, np.uint8).ravel() for x in seeds])
+        self.L.cl_queue_seeds(s, len(s) // 32)
+
+    def load_model(self, path):
+        m = self.L.cl_load_model(path.encode())
+        if not m:
+            raise FileNotFoundError(path)
+        k, t = C.c_int(0), C.c_int(0)
+        self.L.cl_model_info(m, C.byref(k), C.byref(t))
+        k, t = k.value, t.value
+        arrays = {"label": np.zeros(k, np.int32), "nsv": np.zeros(k, np.int32),
+                  "rho": np.zeros(k * (k - 1) // 2), "coef": np.zeros((k - 1, t)),
+                  "sv": np.zeros((t, self.l), np.uint32)}
+        self.L.cl_model_arrays(m, *(arrays[a].ctypes.data for a in ("label", "nsv", "rho", "coef", "sv")))
+        return m, arrays
+
+    def setup(self, seed_a, seed_e):
+        mpk = np.zeros((self.l + 1, 3, self.n), np.uint32)
+        msk = np.zeros((self.l, 3, self.n), np.uint32)
+        self.seeds(seed_a, seed_e)
+        self.L.cl_setup(mpk, msk)
+        return mpk, msk
+
+    def encrypt(self, x, mpk, seed2):
+        c = np.zeros((self.l + 1, 3, self.n), np.uint32)
+        self.seeds(seed2)
+        self.L.cl_encrypt(np.ascontiguousarray(x, np.uint32), np.ascontiguousarray(mpk, np.uint32).copy(), c)
+        return c
+
+    def predict(self, model, c, msk, pairs, total_sv, gpu=False):
+        """(label, dec[pairs], kvalue[total_sv]) of svm_predict_cpu (gpu: svm_predict_gpu)"""
+        dec = np.zeros(pairs)
+        kvalue = np.zeros(total_sv)
+        f = self.L.cl_predict_gpu if gpu else self.L.cl_predict_cpu
+        label = f(model, np.ascontiguousarray(c, np.uint32), np.ascontiguousarray(msk, np.uint32), dec, kvalue)
+        return label, dec, kvalue

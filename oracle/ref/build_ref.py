@@ -175,6 +175,53 @@ def build_modeb(root, force=False):
     return lib
 
 
+# --------------------------------------------------------------- the reference's own callers
+CALLERS_VARIANT = ("n2048_l124", (2048, 124))
+
+
+def build_callers(root, force=False):
+    """oracle/_ref/callers/libcallers.so: the reference's callers of the GPU entry points
+    (main.c with main renamed, src/*.c including rlwe_sife.c's *_gui wrappers, svm/svm.cpp)
+    compiled unmodified at n = 2048, l = 124 and linked against cufe_b200/libcufe_b200.so,
+    which must resolve rlwe_sife_{setup,encrypt,keygen}_gpu and rlwe_sife_decrypt_gmp_gpu
+    (the link fails otherwise).  Requires the library to be built first."""
+    name, dims = CALLERS_VARIANT
+    d = os.path.join(OUT, "callers")
+    lib = os.path.join(d, "libcallers.so")
+    cufe_dir = os.path.join(os.path.dirname(ORACLE), "cufe_b200")
+    cufe_lib = os.path.join(cufe_dir, "libcufe_b200.so")
+    if not os.path.exists(cufe_lib):
+        raise FileNotFoundError(cufe_lib + " (build the library first)")
+    if os.path.exists(lib) and not force and os.path.getmtime(lib) >= os.path.getmtime(cufe_lib):
+        return lib
+    os.makedirs(d, exist_ok=True)
+    gen_headers(dims[0], dims[1], d)
+    src_dir = os.path.join(root, "src")
+    pre = ["-include", os.path.join(d, "gen_params.h")]
+    inc = ["-I", src_dir, "-I", root, "-I", os.path.join(HERE, "shim")]
+    objs = []
+    units = [os.path.join(src_dir, u) for u in UNITS]
+    units += [os.path.join(root, "main.c"), os.path.join(HERE, "callers_glue.c")]
+    for src in units:
+        obj = os.path.join(d, os.path.basename(src) + ".o")
+        extra = list(pre)
+        if src.endswith("ntt.c"):
+            extra += ["-include", os.path.join(d, "gen_consts.h")]
+        if src.endswith("main.c"):
+            extra += ["-Dmain=ref_main"]
+        subprocess.run(["gcc", "-c", src, "-o", obj] + CFLAGS + extra + inc, check=True)
+        objs.append(obj)
+    svm_obj = os.path.join(d, "svm.o")
+    subprocess.run(["g++", "-c", os.path.join(root, "svm", "svm.cpp"), "-o", svm_obj, "-O3", "-fPIC", "-w"],
+                   check=True)
+    objs.append(svm_obj)
+    link = (["g++", "-shared", "-o", lib] + objs +
+            ["-L", cufe_dir, "-l:libcufe_b200.so", "-Wl,-rpath,$ORIGIN/../../../cufe_b200",
+             "-Wl,--wrap=malloc", "-Wl,--wrap=free", "-Wl,--no-undefined", "-l:libgmp.so.10", "-lm"])
+    subprocess.run(link, check=True)
+    return lib
+
+
 def build_all(root=None, force=False):
     root = ref_root(root)
     if not os.path.isdir(os.path.join(root, "src")):
@@ -182,6 +229,7 @@ def build_all(root=None, force=False):
     for name, dims in VARIANTS.items():
         build_variant(root, name, dims, force)
     build_modeb(root, force)
+    build_callers(root, force)
     return True
 
 

@@ -4,7 +4,8 @@ The reference (cuFE src/*.c) is compiled unmodified by oracle/ref/build_ref.py i
 oracle/_ref/<variant>/libref.so; this script drives that build with fixed seeds and stores
 its outputs.  Run in the build container (needs the reference tree):
 
-    python oracle/build.py && python tests/golden/make_golden.py
+    python oracle/build.py && python oracle/ref/build_ref.py --root <reference tree> &&
+    python tests/golden/make_golden.py <reference tree>
 
 Outputs:
   ref_n256_l8.npz   full arrays at n=256, l=8: NTT/INTT vectors, AES-CTR streams, sampler
@@ -16,6 +17,17 @@ Outputs:
                     from an AES context it never initialises; the keyed ciphertext is the
                     reference's ciphertext with its zero-key f_i replaced by the reference
                     sampler's keyed stream, exact since c_i is linear in f_i)
+  ref_svm_a1a.npz   svm_predict5's path end to end on the reference's shipped model and test
+                    set (svm model/a1a.txt.model, a1a.t): the model's arrays as main.c reads
+                    them, the 200 test vectors main.c's predict() classifies first (lines
+                    101-300: it skips the first 100), the setup and encryption seeds, and per
+                    vector the label and decision value of the reference's svm_predict_cpu
+                    (main.c:137-267: per support vector keygen, decrypt, GMP decode, vote),
+                    run at n = 2048, l = 124 by oracle/_ref/callers/libcallers.so
+  ref_svm_small.npz the same prediction on a synthetic three-class model with classes of 1, 3
+                    and 6 support vectors (the vote's term loops at odd and even short
+                    lengths), written in libsvm's format and read by the reference's own
+                    svm_load_model, 12 test vectors
   ref_modeb.npz     the GPU counter-to-sample mapping (mode B) from the reference's own kernel
                     bodies (src/sample_gpu.cu) run on the host by oracle/_ref/modeb/libmodeb.so:
                     polynomial 0 (the first 4096 samples) per sigma for two keys as signed
@@ -32,7 +44,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.ffi import Q, Reference, ReferenceModeB  # noqa: E402
+from oracle.ffi import Q, Reference, ReferenceCallers, ReferenceModeB  # noqa: E402
+
+SVM_ROWS = 200
+
+
+def ref_root():
+    root = os.environ.get("CUFE_REFERENCE_ROOT") or (sys.argv[1] if len(sys.argv) > 1 else None)
+    if not root:
+        raise SystemExit("usage: make_golden.py <reference tree> (or set CUFE_REFERENCE_ROOT)")
+    return root
 
 
 def canon(a):
@@ -126,8 +147,96 @@ def modeb():
     np.savez_compressed(os.path.join(HERE, "ref_modeb.npz"), **out)
 
 
+def svm_small():
+    import tempfile
+    sys.path.insert(0, ROOT)
+    from cufe_b200 import libsvm
+    R = ReferenceCallers()
+    rng = np.random.default_rng(0xC0FE0301)
+    nsv = np.array([1, 3, 6], np.int32)
+    sv = np.zeros((int(nsv.sum()), R.l), np.uint32)
+    for i in range(len(sv)):
+        sv[i, rng.choice(np.arange(1, R.l), 14, replace=False)] = 1
+    coef = rng.uniform(-1, 1, (2, len(sv)))
+    rho = rng.uniform(-0.5, 0.5, 3)
+    label = np.array([5, -2, 9], np.int32)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "small.model")
+        libsvm.save_model(path, 3, sv, nsv, coef, rho, label)
+        model, arr = R.load_model(path)
+    assert (arr["sv"] == sv).all() and (arr["coef"] == coef).all() and (arr["rho"] == rho).all()
+    seed_a, seed_e = rng.integers(0, 256, (2, 32), dtype=np.uint8)
+    mpk, msk = R.setup(seed_a, seed_e)
+    x = np.zeros((12, R.l), np.uint32)
+    for t in range(12):
+        x[t, rng.choice(np.arange(1, R.l), 14, replace=False)] = 1
+    seeds2 = rng.integers(0, 256, (12, 32), dtype=np.uint8)
+    labels, decs, kvs = [], [], []
+    for t in range(12):
+        lab, dec, kv = R.predict(model, R.encrypt(x[t], mpk, seeds2[t]), msk, 3, len(sv))
+        labels.append(lab)
+        decs.append(dec)
+        kvs.append(kv)
+    R.L.cl_free_model(model)
+    np.savez_compressed(os.path.join(HERE, "ref_svm_small.npz"), n=R.n, l=R.l, label=label, nsv=nsv, rho=rho,
+                        coef=coef, sv=sv.astype(np.uint8), x=x.astype(np.uint8), seed_a=seed_a, seed_e=seed_e,
+                        seeds2=seeds2, ref_label=np.array(labels), ref_dec=np.array(decs),
+                        ref_kvalue=np.array(kvs).astype(np.uint16))
+
+
+def _svm_init(model_path, seed_a, seed_e):
+    global _R, _M, _MSK, _MPK
+    _R = ReferenceCallers()
+    _M, _ = _R.load_model(model_path)
+    _MPK, _MSK = _R.setup(seed_a, seed_e)
+
+
+def _svm_one(args):
+    x, seed2 = args
+    c = _R.encrypt(x, _MPK, seed2)
+    label, dec, kv = _R.predict(_M, c, _MSK, 1, 591)
+    return label, dec, _R.L.cl_predict_plain(_M, np.ascontiguousarray(x, np.uint32)), kv
+
+
+def svm(root):
+    import multiprocessing as mp
+    model_path = os.path.join(root, "svm model", "a1a.txt.model")
+    R = ReferenceCallers()
+    model, arr = R.load_model(model_path)
+    R.L.cl_free_model(model)
+    assert len(arr["label"]) == 2 and len(arr["sv"]) == 591, "written for the two-class a1a model"
+    rows, target = [], []
+    with open(os.path.join(root, "svm model", "a1a.t")) as f:
+        for g, line in enumerate(f, 1):
+            if g <= 100:  # main.c's predict() skips the first 100 lines
+                continue
+            parts = line.split()
+            x = np.zeros(R.l, np.uint32)
+            for tok in parts[1:]:
+                i, v = tok.split(":")
+                x[int(i)] = int(float(v))
+            rows.append(x)
+            target.append(int(float(parts[0])))
+            if len(rows) == SVM_ROWS:
+                break
+    rng = np.random.default_rng(0xC0FE0300)
+    seed_a, seed_e = rng.integers(0, 256, (2, 32), dtype=np.uint8)
+    seeds2 = rng.integers(0, 256, (SVM_ROWS, 32), dtype=np.uint8)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1), _svm_init, (model_path, seed_a, seed_e)) as pool:
+        res = pool.map(_svm_one, list(zip(rows, seeds2)), chunksize=4)
+    np.savez_compressed(os.path.join(HERE, "ref_svm_a1a.npz"), n=R.n, l=R.l, label=arr["label"], nsv=arr["nsv"],
+                        rho=arr["rho"], coef=arr["coef"], sv=arr["sv"].astype(np.uint8),
+                        x=np.stack(rows).astype(np.uint8), target=np.array(target, np.int8), seed_a=seed_a,
+                        seed_e=seed_e, seeds2=seeds2, ref_label=np.array([r[0] for r in res]),
+                        ref_dec=np.array([r[1] for r in res]), plain_label=np.array([r[2] for r in res]),
+                        ref_kvalue=np.array([r[3] for r in res]).astype(np.uint16))
+
+
 if __name__ == "__main__":
+    root = ref_root()
     small()
     c2()
     modeb()
+    svm(root)
+    svm_small()
     print("golden fixtures written to", HERE)

@@ -8,6 +8,10 @@ decoded inner product equal to the plaintext dot product mod p_i.  Also: several
 the same results as one, and a CUDA-graph replay equals an eager step, including after new
 seeds are written into the bound buffers.
 """
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -100,3 +104,50 @@ def test_batch_graph_replay(rng, oracle_built):
         assert int(rep[0][i]) % (64 * l + 1) == int(xs[i] @ ys[i]) % (64 * l + 1)
     B.status()
     B.close()
+
+
+def test_batch_real_sizes_and_chunk_boundaries(oracle_built):
+    """instances of the heterogeneous-batch shapes (n 2048/4096, l up to 1024); instance 0 is the
+    reference's C2 golden round (n 4096, l 784, its seeds and x; f_i keyed by seed3).  One chunk:
+    instance 0's ciphertext has the reference's hash, the others equal the oracle's encryption.
+    One instance per chunk (chunks hold whole instances, so every boundary falls between two
+    instances' streams): the same outputs as one chunk.  Every inner product is checked."""
+    doc = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_c2.json")))
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    ns, ls = [4096, 2048, 4096, 2048, 4096], [784, 1024, 1024, 33, 300]
+    rng = np.random.default_rng(0xC0FE0500)
+    cnt = len(ns)
+    sa, se, s2, s3 = (seeds(rng, cnt) for _ in range(4))
+    gr = np.random.default_rng(0xC0FE0002)  # the golden round's seeds, then x
+    g_a, g_e, g_2 = gr.integers(0, 256, (3, 32), dtype=np.uint8)
+    sa[0], se[0], s2[0], s3[0] = g_a, g_e, g_2, np.array(doc["seed3"], np.uint8)
+    xs = [gr.integers(0, 5, 784, dtype=np.uint32).astype(np.int64)]
+    xs += [rng.integers(0, 5, l, dtype=np.int64) for l in ls[1:]]
+    ys = [rng.integers(-16, 17, l, dtype=np.int64) for l in ls]
+    results = []
+    for chunk in (0, 1):  # 0: one chunk (default budget); 1 byte: one instance per chunk
+        B = cf.Batch(ns, ls, max_chunk_bytes=chunk)
+        assert B.chunks == (1 if chunk == 0 else cnt)
+        B.setup(sa, None, se)
+        x = dev(B.pack(xs).astype(np.uint32))
+        y = dev(B.pack(ys).astype(np.int32))
+        d0 = dev(np.zeros((cnt, 3), np.uint32))
+        out = B.bind(x, y, cf.bytes_to_dev(s2), cf.bytes_to_dev(s3), d0=d0)
+        B.run()
+        torch.cuda.synchronize()
+        B.status()
+        results.append((cf.u32(out).copy(), cf.u32(d0).copy()))
+        if chunk == 0:
+            ct0 = B.fetch(B.instance(0)[3], 785 * 3 * 4096)
+            assert sha(ct0) == doc["ct_keyed"]
+            for i in (1, 2, 3):
+                n, l = ns[i], ls[i]
+                O = Oracle(n, l)
+                rmpk, _ = O.setup(sa[i], None, se[i])
+                rct = O.encrypt(xs[i].astype(np.uint32), rmpk, s2[i], s3[i])
+                assert (B.fetch(B.instance(i)[3], (l + 1) * 3 * n).reshape(l + 1, 3, n) == canon(rct)).all(), i
+        B.close()
+    assert (results[0][0] == results[1][0]).all() and (results[0][1] == results[1][1]).all()
+    for i, l in enumerate(ls):
+        p = 64 * l + 1
+        assert int(results[0][0][i]) % p == int(xs[i] @ ys[i]) % p, i

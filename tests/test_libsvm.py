@@ -6,7 +6,9 @@ import pytest
 
 from cufe_b200 import libsvm
 
-REF_MODEL = "/root/reference/svm model/a1a.txt.model"
+REF_ROOT = os.environ.get("CUFE_REFERENCE_ROOT")
+REF_MODEL = os.path.join(REF_ROOT, "svm model", "a1a.txt.model") if REF_ROOT else ""
+GOLD_SVM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_svm_a1a.npz")
 
 
 def test_round_trip_integer_model(tmp_path, rng):
@@ -45,11 +47,24 @@ def test_rejects_nonlinear(tmp_path):
         libsvm.to_integer(libsvm.load_model(p), 4)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MODEL), reason="reference tree not present")
+def test_reference_model_arrays_round_trip(tmp_path):
+    """the arrays the reference's own svm_load_model read from its a1a model (fixture) survive
+    this module's writer and parser unchanged"""
+    g = np.load(GOLD_SVM)
+    p = str(tmp_path / "a1a.model")
+    libsvm.save_model(p, 2, g["sv"], g["nsv"], g["coef"], g["rho"], g["label"])
+    sv, nsv, coef, rho, label, scale = libsvm.to_integer(libsvm.load_model(p), int(g["l"]))
+    assert scale == 1.0 and (sv == g["sv"]).all() and (nsv == g["nsv"]).all()
+    assert (coef == g["coef"]).all() and (rho == g["rho"]).all() and (label == g["label"]).all()
+
+
+@pytest.mark.skipif(not os.path.exists(REF_MODEL), reason="CUFE_REFERENCE_ROOT not set")
 def test_reference_model_parses():
-    """the reference's bundled linear model (read in place, nothing copied)"""
+    """the reference's bundled linear model, read in place: this parser gives the arrays the
+    reference's svm_load_model gave (fixture)"""
     m = libsvm.load_model(REF_MODEL)
     assert m["kernel_type"] == "linear" and m["nr_class"] == 2
     assert m["total_sv"] == int(m["nr_sv"].sum())
     sv, nsv, coef, rho, label, scale = libsvm.to_integer(m, 124)
-    assert scale == 1.0 and sv.min() >= 0 and sv.max() <= 16
+    g = np.load(GOLD_SVM)
+    assert scale == 1.0 and (sv == g["sv"]).all() and (coef == g["coef"]).all() and (rho == g["rho"]).all()
