@@ -315,6 +315,9 @@ def gpu_arm(args):
         ctx.decrypt(ct, y_dev, sky, y_signed=True, dy=dy)
         ctx.decode(dy, out=out)
 
+    # the encryption shape for this batch size, chosen by the library's tuner (bit-exact either way)
+    b0 = first(0)
+    enc_group, enc_ms = ctx.tune_encrypt(x_dev[b0:b0 + B], mpk, seeds2[b0:b0 + B], seeds3[b0:b0 + B], ct=ct)
     for w in range(warm):
         step(w, scratch)
     ctx.sync()
@@ -386,6 +389,7 @@ def gpu_arm(args):
 
     # --- batched with the constant-coefficient decrypt (decrypt + decode of coefficient 0 only)
     r0 = torch.empty((steps, B, 1), dtype=torch.int32, device=dev)
+    c0_form, c0_tune_ms = ctx.tune_decrypt_coef0(ct, y_dev, sky, y_signed=True, out=r0[0])
     torch.cuda.synchronize()
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g0.record(stream)
@@ -491,6 +495,11 @@ def gpu_arm(args):
                         "points, one call per encryption, host buffers: plain_dropin); this library's own "
                         "device-resident batch-1 form is bounded near 2.2x by the sigma_3 keystream work "
                         "that every encryption carries"},
+            "tuning": {"encrypt_instances_per_group": enc_group, "encrypt_ms_by_group": enc_ms,
+                       "coef0_form": c0_form, "coef0_ms_by_form": c0_tune_ms,
+                       "coef0_forms": ["per pair", "64x32", "64x64", "32x32", "32x64"],
+                       "note": "shapes chosen by the library's tuners (cufe_tune_encrypt, cufe_tune_decrypt_coef0) "
+                               "on this workload before timing; every form gives the same bits"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
             "clocks": clocks}
@@ -737,7 +746,7 @@ def batched_mixed(args):
     return 0 if line["bit_exact"] else 1
 
 
-def mixed_measure(count, steps, warmup, chunk_gb):
+def mixed_measure(count, steps, warmup, chunk_gb, tune_gb=(12, 24, 36)):
     """Heterogeneous batch: `count` independent IPFE instances, l = round(exp(U[ln 32, ln 1024])),
     N in {2048, 4096} 50/50, x in [0, 4], y in [-16, 16]; instance i's data from
     SplitMix64(0xC0FE0003 + i).  Keys are generated once (setup timed separately) and stay
@@ -777,6 +786,9 @@ def mixed_measure(count, steps, warmup, chunk_gb):
         s2.copy_(host_seeds[k, 0], non_blocking=True)
         s3.copy_(host_seeds[k, 1], non_blocking=True)
 
+    seeds_in(0)
+    budgets = [b << 30 for b in tune_gb] if tune_gb else []
+    chunk_choice = B.tune(budgets) if budgets else (chunk_gb << 30, [])
     for k in range(warmup):
         seeds_in(k)
         B.replay()
@@ -827,6 +839,8 @@ def mixed_measure(count, steps, warmup, chunk_gb):
                                    "replay per step" % count,
                        "instances": count, "mean_l": float(np.mean(ls)), "n4096_share": float(np.mean(np.array(ns) == 4096)),
                        "chunks": B.chunks, "key_gb": B.key_bytes / 1e9, "scratch_gb": B.scratch_bytes / 1e9,
+                       "chunk_budget_gb": chunk_choice[0] / (1 << 30),
+                       "chunk_tuning_ms": dict(zip([str(b) for b in tune_gb], chunk_choice[1])) if budgets else None,
                        "sigma3_samples_per_step": samples},
             "sigma3_samples_per_s": samples / (ms / steps / 1000.0), "clocks": clocks}
     B.close()
@@ -1058,6 +1072,8 @@ def svm_workload(args):
         c.encrypt(xd, mpk, s2[k], None, ct=ct)
         m.predict(ct, labels=out, kvalue=kvo)
 
+    c.encrypt(xd, mpk, s2[0], None, ct=ct)
+    svm_form, svm_form_ms = m.tune(ct)  # the coefficient-0 decrypt form for 1,000 x 500 pairs
     for k in range(args.warmup):
         step(k, labels[0], kv)
     c.sync()
@@ -1089,6 +1105,8 @@ def svm_workload(args):
             "value": preds, "unit": "predictions/s", "ip_per_s": preds * nsv, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "uint32",
             "data": "synthetic", "bit_exact": ok, "sv_keys_s": keys_s,
+            "tuning": {"coef0_form": svm_form, "coef0_ms_by_form": svm_form_ms,
+                       "coef0_forms": ["per pair", "64x32", "64x64", "32x32", "32x64"]},
             "config": {"workload": "1,000 test vectors (a1a-shaped) x 500 support vectors, encrypt + predict per step",
                        "n": n, "l": l, "test_vectors": ntest, "support_vectors": nsv},
             "gpu_launches": svm_launches, "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},

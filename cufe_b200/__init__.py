@@ -65,6 +65,11 @@ def lib():
             "cufe_decrypt": [vp, i, vp, i, vp, i, vp, vp, vp],
             "cufe_decrypt_noalloc": [vp, vp, i, vp, i, vp, vp, vp],
             "cufe_decode": [vp, i, vp, i, vp, vp],
+            "cufe_tune_encrypt": [vp, i, vp, vp, vp, vp, vp, vp, vp, vp],
+            "cufe_tune_decrypt_coef0": [vp, i, vp, i, vp, i, vp, vp, vp, vp, vp],
+            "cufe_decrypt_coef0_form": [vp, i, i, vp, i, vp, i, vp, vp, vp, vp],
+            "cufe_svm_tune": [vp, i, vp, vp, vp, vp],
+            "cufe_batch_tune": [vp, i, vp, vp, vp, vp],
             "cufe_decrypt_coef0": [vp, i, vp, i, vp, i, vp, vp, vp, vp],
             "cufe_sample_cpu_map": [vp, i, i, vp, i, vp, vp],
             "cufe_sample_gpu_map": [vp, i, vp, i, i, vp, vp],
@@ -327,6 +332,35 @@ class Context:
                                           _stream(stream, self.device)), "cufe_decrypt_noalloc")
         return dy
 
+    def tune_encrypt(self, x, mpk, seeds2, seeds3, ct=None, stream=None):
+        """time one and two instances per thread group for this batch size on these inputs (the
+        ciphertexts land in ct either way); the context keeps the faster.  -> (choice, [ms1, ms2])"""
+        batch = x.shape[0]
+        ct = self.ct_buf(batch) if ct is None else ct
+        s2, s3 = _seeds(seeds2), _seeds(seeds3)
+        ch, ms = C.c_int(0), (C.c_float * 2)()
+        _check(lib().cufe_tune_encrypt(self.h, batch, _ptr(x), _ptr(mpk), _ptr(s2), _ptr(s3), _ptr(ct), C.byref(ch),
+                                       ms, _stream(stream, self.device)), "cufe_tune_encrypt")
+        return ch.value, list(ms)
+
+    def tune_decrypt_coef0(self, ct, y, sky, y_signed=False, out=None, stream=None):
+        """time the five coefficient-0 decrypt forms for (nct, nkeys); -> (form, ms[5])"""
+        nct, nkeys = ct.shape[0], y.shape[0]
+        out = _dev((nct, nkeys), self.dev) if out is None else out
+        ch, ms = C.c_int(0), (C.c_float * 5)()
+        _check(lib().cufe_tune_decrypt_coef0(self.h, nct, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky), _ptr(out),
+                                             C.byref(ch), ms, _stream(stream, self.device)), "cufe_tune_decrypt_coef0")
+        return ch.value, list(ms)
+
+    def decrypt_coef0_form(self, form, ct, y, sky, y_signed=False, d0=None, out=None, stream=None):
+        """decrypt_coef0 in a given form (0 per pair, 1..4 tile shapes)"""
+        nct, nkeys = ct.shape[0], y.shape[0]
+        out = _dev((nct, nkeys), self.dev) if out is None else out
+        _check(lib().cufe_decrypt_coef0_form(self.h, form, nct, _ptr(ct), nkeys, _ptr(y), int(y_signed), _ptr(sky),
+                                             _ptr(d0), _ptr(out), _stream(stream, self.device)),
+               "cufe_decrypt_coef0_form")
+        return out
+
     def decrypt_coef0(self, ct, y, sky, y_signed=False, d0=None, out=None, stream=None):
         """decrypt and decode coefficient 0 of every (ciphertext, key) pair: out[nct][nkeys]"""
         nct, nkeys = ct.shape[0], y.shape[0]
@@ -505,6 +539,19 @@ class Batch:
     def replay(self, stream=None):
         _check(lib().cufe_batch_replay(self.h, _stream(stream, self.device)), "cufe_batch_replay")
 
+    def tune(self, budgets, stream=None):
+        """re-chunk at each scratch budget (bytes), time an eager step, keep the fastest;
+        -> (chosen budget, ms per budget, -1 where it did not fit)"""
+        b = (C.c_size_t * len(budgets))(*budgets)
+        ms = (C.c_float * len(budgets))()
+        chosen = C.c_size_t(0)
+        _check(lib().cufe_batch_tune(self.h, len(budgets), b, C.byref(chosen), ms, _stream(stream, self.device)),
+               "cufe_batch_tune")
+        ch, kb, sb = C.c_int(0), C.c_size_t(0), C.c_size_t(0)
+        _check(lib().cufe_batch_info(self.h, None, C.byref(ch), C.byref(kb), C.byref(sb)), "cufe_batch_info")
+        self.chunks, self.scratch_bytes = ch.value, sb.value
+        return chosen.value, list(ms)
+
     def profile(self, on):
         """kernel timing of eager steps (run()); on clears the totals"""
         _check(lib().cufe_batch_profile(self.h, int(on)), "cufe_batch_profile")
@@ -670,6 +717,13 @@ class SvmModel:
         _check(lib().cufe_svm_predict(self.h, nct, _ptr(ct), _ptr(labels), _ptr(kvalue), _ptr(dec),
                                       _stream(stream, self.ctx.device)), "cufe_svm_predict")
         return labels
+
+    def tune(self, ct, stream=None):
+        """pick the coefficient-0 decrypt form for this many test vectors; -> (form, ms[5])"""
+        ch, ms = C.c_int(0), (C.c_float * 5)()
+        _check(lib().cufe_svm_tune(self.h, ct.shape[0], _ptr(ct), C.byref(ch), ms, _stream(stream, self.ctx.device)),
+               "cufe_svm_tune")
+        return ch.value, list(ms)
 
     def close(self):
         if getattr(self, "h", None):

@@ -238,7 +238,11 @@ struct Batch {
   ModQ mq{};
   DecodeArgs dd{};
 
+  size_t chunk_budget = 0;       // scratch budget the chunks were laid out for
+  uint64_t sky_words = 0;
   int create(int count_, const int *n_, const int *l_, size_t max_chunk_bytes, int dev);
+  int layout(size_t max_chunk_bytes);
+  int tune(int nb, const size_t *budgets, size_t *chosen, float *ms, cudaStream_t s);
   void release();
   int setup(const uint8_t *sa, const uint8_t *ss, const uint8_t *se, cudaStream_t s);
   int run(cudaStream_t s);
@@ -325,7 +329,28 @@ int Batch::create(int count_, const int *n_, const int *l_, size_t max_chunk_byt
     max_l = std::max(max_l, I.l);
   }
   key_bytes = kw * 4;
-  // chunks: greedy in internal order under the scratch budget
+  sky_words = skw;
+  int rc = layout(max_chunk_bytes);
+  if (rc) return rc;
+  CUFE_CUDA(cudaMalloc(&keys, std::max<size_t>(key_bytes, 256)));
+  CUFE_CUDA(cudaMalloc(&sky, std::max<size_t>(sky_words * 4, 256)));
+  CUFE_CUDA(cudaMalloc(&rk, (size_t)2 * count * 60 * 4));
+  CUFE_CUDA(cudaMalloc(&perm, (size_t)count * 4));
+  CUFE_CUDA(cudaMemcpy(perm, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice));
+  CUFE_CUDA(cudaMalloc(&status, 256));
+  CUFE_CUDA(cudaMemset(status, 0, 256));
+  return CUFE_OK;
+}
+
+// Chunks (greedy in internal order under the scratch budget), their tables and the step
+// scratch; keys and bound buffers are untouched, so a batch can be re-chunked at any time.
+int Batch::layout(size_t max_chunk_bytes) {
+  drop_graph();
+  if (tables) cudaFree(tables);
+  if (scratch) cudaFree(scratch);
+  tables = scratch = nullptr;
+  chunks.clear();
+  chunk_budget = max_chunk_bytes;
   auto inst_bytes = [&](const InstDev &I) {
     const uint64_t poly = (uint64_t)3 * I.n * 4;
     const uint64_t R3 = cpu_map_refills(I.l, I.n, 2), R2 = cpu_map_refills(2, I.n, 1);
@@ -424,16 +449,58 @@ int Batch::create(int count_, const int *n_, const int *l_, size_t max_chunk_byt
   a_ct = a_f3 + a256(m_f3);
   a_samp = a_ct + a256(m_ct);
   scratch_bytes = a_samp + a256(m_samp);
-  CUFE_CUDA(cudaMalloc(&keys, std::max<size_t>(key_bytes, 256)));
-  CUFE_CUDA(cudaMalloc(&sky, std::max<size_t>(skw * 4, 256)));
   CUFE_CUDA(cudaMalloc(&tables, std::max<size_t>(blob.size(), 256)));
   CUFE_CUDA(cudaMemcpy(tables, blob.data(), blob.size(), cudaMemcpyHostToDevice));
-  if (!keys_only) CUFE_CUDA(cudaMalloc(&scratch, scratch_bytes));
-  CUFE_CUDA(cudaMalloc(&rk, (size_t)2 * count * 60 * 4));
-  CUFE_CUDA(cudaMalloc(&perm, (size_t)count * 4));
-  CUFE_CUDA(cudaMemcpy(perm, order.data(), (size_t)count * 4, cudaMemcpyHostToDevice));
-  CUFE_CUDA(cudaMalloc(&status, 256));
-  CUFE_CUDA(cudaMemset(status, 0, 256));
+  if (!keys_only) {
+    if (cudaMalloc(&scratch, scratch_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      scratch = nullptr;
+      set_last_error("batch: no room for " + std::to_string(scratch_bytes) + " B of step scratch");
+      return CUFE_ERR_NOMEM;
+    }
+  }
+  ran = false;
+  return CUFE_OK;
+}
+
+// Times one eager step at each scratch budget (the bound buffers must be set), keeps the
+// fastest layout.  A budget whose scratch does not fit the device is skipped (ms = -1).
+int Batch::tune(int nb, const size_t *budgets, size_t *chosen, float *ms, cudaStream_t s) {
+  if (nb < 1 || !budgets || !x || !y || !seeds2 || !seeds3 || !out) return CUFE_ERR_INVALID;
+  const size_t before = chunk_budget;
+  int best = -1;
+  float best_ms = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (ms) ms[i] = -1.0f;
+    if (!budgets[i]) continue;
+    int rc = layout(budgets[i]);
+    if (rc == CUFE_ERR_NOMEM) continue;
+    if (rc) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUFE_CUDA(cudaEventCreate(&e0));
+    CUFE_CUDA(cudaEventCreate(&e1));
+    float t = 0;
+    rc = run(s);  // untimed: first use of this layout
+    if (!rc && cudaEventRecord(e0, s) == cudaSuccess) rc = run(s);
+    const bool ok = !rc && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+                    cudaEventElapsedTime(&t, e0, e1) == cudaSuccess;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (!ok) {
+      set_last_error("batch tune: event timing failed");
+      return CUFE_ERR_CUDA;
+    }
+    if (ms) ms[i] = t;
+    if (best < 0 || t < best_ms) best = i, best_ms = t;
+  }
+  const int rc = layout(best >= 0 ? budgets[best] : before);
+  if (rc) return rc;
+  if (best < 0) {
+    set_last_error("batch tune: no budget fits the device");
+    return CUFE_ERR_NOMEM;
+  }
+  if (chosen) *chosen = budgets[best];
   return CUFE_OK;
 }
 
@@ -1172,6 +1239,13 @@ int cufe_batch_run(cufe_batch *h, void *stream) {
   const int rc = h->b.run(static_cast<cudaStream_t>(stream));
   cufe::t_prof = nullptr;
   return rc;
+}
+
+int cufe_batch_tune(cufe_batch *h, int ncand, const size_t *budgets, size_t *chosen, float *ms, void *stream) {
+  if (!h || h->b.keys_only) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  if (cudaSetDevice(h->b.device) != cudaSuccess) return CUFE_ERR_CUDA;
+  return h->b.tune(ncand, budgets, chosen, ms, static_cast<cudaStream_t>(stream));
 }
 
 int cufe_batch_profile(cufe_batch *h, int on) {

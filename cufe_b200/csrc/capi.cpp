@@ -207,6 +207,26 @@ int cufe_decrypt_coef0(cufe_ctx *h, int nct, const uint32_t *d_ct, int nkeys, co
   CTX_CALL(h, cufe::ctx_decrypt_coef0(h->c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d_d0, d_out, h->c.pick(stream)));
 }
 
+int cufe_decrypt_coef0_form(cufe_ctx *h, int form, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y,
+                            int y_signed, const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, void *stream) {
+  if (!d_ct || !d_y || !d_sky || !d_out) return CUFE_ERR_INVALID;
+  CTX_CALL(h, cufe::ctx_decrypt_coef0_form(h->c, form, nct, d_ct, nkeys, d_y, y_signed, d_sky, d_d0, d_out,
+                                           h->c.pick(stream)));
+}
+
+int cufe_tune_decrypt_coef0(cufe_ctx *h, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                            const uint32_t *d_sky, uint32_t *d_out, int *choice, float *ms, void *stream) {
+  if (!d_ct || !d_y || !d_sky || !d_out) return CUFE_ERR_INVALID;
+  CTX_CALL(h, cufe::ctx_tune_decrypt_coef0(h->c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d_out, choice, ms,
+                                           h->c.pick(stream)));
+}
+
+int cufe_tune_encrypt(cufe_ctx *h, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                      const uint8_t *seeds3, uint32_t *d_ct, int *choice, float *ms, void *stream) {
+  if (!d_x || !d_mpk || !seeds2 || !d_ct) return CUFE_ERR_INVALID;
+  CTX_CALL(h, cufe::ctx_tune_encrypt(h->c, batch, d_x, d_mpk, seeds2, seeds3, d_ct, choice, ms, h->c.pick(stream)));
+}
+
 int cufe_decode(cufe_ctx *h, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_out, void *stream) {
   if (!d_dy || !d_out) return CUFE_ERR_INVALID;
   CTX_CALL(h, cufe::ctx_decode(h->c, count, d_dy, ncoeff, d_out, h->c.pick(stream)));
@@ -369,6 +389,12 @@ int cufe_svm_predict(cufe_svm *sm, int nct, const uint32_t *d_ct, int *d_label, 
   if (!sm) return CUFE_ERR_INVALID;
   cufe_ctx *h = sm->ctx;
   CTX_CALL(h, cufe::svm_predict(h->c, *sm->m, nct, d_ct, d_label, d_kvalue, d_dec, h->c.pick(stream)));
+}
+
+int cufe_svm_tune(cufe_svm *sm, int nct, const uint32_t *d_ct, int *choice, float *ms, void *stream) {
+  if (!sm || !d_ct) return CUFE_ERR_INVALID;
+  cufe_ctx *h = sm->ctx;
+  CTX_CALL(h, cufe::svm_tune(h->c, *sm->m, nct, d_ct, choice, ms, h->c.pick(stream)));
 }
 
 int cufe_svm_destroy(cufe_svm *sm) {

@@ -3,8 +3,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cufe_internal.cuh"
@@ -43,6 +45,11 @@ struct Ctx {
   uint32_t *d_status = nullptr;  // sampler status word (device)
   std::mutex mu;                 // serialises host calls on this context
   Prof prof;                     // per-kernel timing (cufe_profile_*)
+  // shapes chosen by the tuners (cufe_tune_*): encryption instances per thread group by batch
+  // size, coefficient-0 decrypt form by (ciphertexts, keys); absent: the fixed rules
+  std::map<int, int> enc_group;
+  std::map<std::pair<int, int>, int> coef0_form;
+  int enc_group_forced = 0;  // set by the encryption tuner while it times one form
 
   int init(int n, int l, int device);
   void release();
@@ -85,10 +92,18 @@ int svm_create(Ctx &c, SvmModel &m, int nr_class, int lsv, const int32_t *sv, in
                const double *sv_coef, const double *rho, const int *label, const uint32_t *d_msk, cudaStream_t s);
 int svm_predict(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kval, double *d_dec,
                 cudaStream_t s);
+int svm_tune(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *choice, float *ms, cudaStream_t s);
 SvmModel *svm_new();
 void svm_delete(SvmModel *m);
 int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                       const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s);
+int ctx_decrypt_coef0_form(Ctx &c, int form, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y,
+                           int y_signed, const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s);
+// the tuners: time every form on the caller's buffers (all bit-exact), keep the fastest in c
+int ctx_tune_encrypt(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                     const uint8_t *seeds3, uint32_t *d_ct, int *choice, float *ms, cudaStream_t s);
+int ctx_tune_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                           const uint32_t *d_sky, uint32_t *d_out, int *choice, float *ms, cudaStream_t s);
 int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,
                        cudaStream_t s);
 int ctx_sample_gpu_map(Ctx &c, int sig, const uint8_t *key, int poly0, int npolys, uint32_t *d_out,

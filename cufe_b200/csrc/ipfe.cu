@@ -682,45 +682,63 @@ __global__ void __launch_bounds__(256)
 // Constant-coefficient decrypt of many (ciphertext, key) pairs as a tiled product over K =
 // l + n: for modulus m = blockIdx.z,
 //   d0[c][key][m] = sum_{k<l} c_k[0] y_k + sum_{t<n} c_l[t] b_t,  b_0 = -s[0], b_t = s[n-t],
-// the negacyclic constant term of c_l * sk_y with its sign folded into the key operand.  A CTA
-// computes 64 ciphertexts x 32 keys, 4 x 2 per thread, from 32-deep K chunks staged in shared
-// memory (A reused 32 times, B 64 times).  Products are exact: a, b < 2^31, so four products
-// sum below 2^64 in one wide multiply-add chain, folded into a 64 + 32-bit accumulator (K < 2^34
-// products); one reduction per pair.
-constexpr int kC0Tm = 64, kC0Tn = 32, kC0Kc = 32;
-constexpr int kCoef0TiledMinKeys = 32;  // fewer keys: one CTA per pair
-__device__ __forceinline__ int c0_swz_a(int kk, int i) { return kk * kC0Tm + (i ^ ((kk & 15) << 2)); }
-__device__ __forceinline__ int c0_swz_b(int kk, int j) { return kk * kC0Tn + (j ^ ((kk & 15) << 1)); }
+// the negacyclic constant term of c_l * sk_y with its sign folded into the key operand.  A CTA of
+// 256 threads computes TM = 16 RI ciphertexts x TN = 16 RJ keys, RI x RJ per thread, from
+// 32-deep K chunks staged in shared memory (A reused TN times, B TM times); the rows are
+// XOR-swizzled in steps of the vector width so that the staging stores spread over the banks.
+// Products are exact: a, b < 2^31, so four products sum below 2^64 in one wide multiply-add
+// chain, folded into a 64 + 32-bit accumulator (K < 2^34 products); one reduction per pair.
+// Tile shapes (ciphertexts x keys): 64 x 32 (the default), 64 x 64, 32 x 32, 32 x 64; the
+// context's tuner picks per (ciphertexts, keys).
+constexpr int kC0Kc = 32;
+constexpr int kCoef0TiledMinKeys = 32;  // fewer keys: one CTA per pair (untuned rule)
+constexpr int kCoef0Forms = 5;          // 0 per pair, 1..4 the tile shapes below
+template <int TM, int R>
+__device__ __forceinline__ int c0_swz(int kk, int i) {
+  return kk * TM + (i ^ ((kk & (TM / R - 1)) * R));
+}
+template <int R>
+__device__ __forceinline__ void c0_row(const uint32_t *p, uint32_t (&v)[R]) {
+  if constexpr (R == 4) {
+    const uint4 t = *reinterpret_cast<const uint4 *>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+    const uint2 t = *reinterpret_cast<const uint2 *>(p);
+    v[0] = t.x, v[1] = t.y;
+  }
+}
 
+template <int RI, int RJ>
 __global__ void __launch_bounds__(256) k_dec_coef0_tiled(const uint32_t *__restrict__ ct, const uint32_t *__restrict__ y,
                                                          int y_signed, int nct, int nkeys,
                                                          const uint32_t *__restrict__ sky, uint32_t *__restrict__ d0,
                                                          SchemeArgs sa) {
-  __shared__ __align__(16) uint32_t As[kC0Kc * kC0Tm];
-  __shared__ __align__(16) uint32_t Bs[kC0Kc * kC0Tn];
+  constexpr int TM = 16 * RI, TN = 16 * RJ;
+  __shared__ __align__(16) uint32_t As[kC0Kc * TM];
+  __shared__ __align__(16) uint32_t Bs[kC0Kc * TN];
   const int m = blockIdx.z, n = sa.ra.n, l = sa.l, K = l + n;
   const uint32_t q = sa.ra.q[m];
   const uint64_t mu = sa.mu[m];
-  const int ct0 = blockIdx.x * kC0Tm, key0 = blockIdx.y * kC0Tn;
+  const int ct0 = blockIdx.x * TM, key0 = blockIdx.y * TN;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  uint64_t lo[4][2];
-  uint32_t hi[4][2];
+  uint64_t lo[RI][RJ];
+  uint32_t hi[RI][RJ];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < RI; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) lo[i][j] = 0, hi[i][j] = 0;
+    for (int j = 0; j < RJ; ++j) lo[i][j] = 0, hi[i][j] = 0;
   for (int k0 = 0; k0 < K; k0 += kC0Kc) {
     // lane-consecutive k: the c_l and sk_y parts are contiguous runs per row
-    for (int e = threadIdx.x; e < kC0Tm * kC0Kc; e += blockDim.x) {
+    for (int e = threadIdx.x; e < TM * kC0Kc; e += blockDim.x) {
       const int i = e / kC0Kc, kk = e % kC0Kc, k = k0 + kk, c = ct0 + i;
       uint32_t a = 0;
       if (k < K && c < nct) {
         const uint32_t *cb = ct + (size_t)c * (l + 1) * 3 * n;
         a = k < l ? cb[((size_t)k * 3 + m) * n] : cb[((size_t)l * 3 + m) * n + (k - l)];
       }
-      As[c0_swz_a(kk, i)] = a;
+      As[c0_swz<TM, RI>(kk, i)] = a;
     }
-    for (int e = threadIdx.x; e < kC0Tn * kC0Kc; e += blockDim.x) {
+    for (int e = threadIdx.x; e < TN * kC0Kc; e += blockDim.x) {
       const int j = e / kC0Kc, kk = e % kC0Kc, k = k0 + kk, key = key0 + j;
       uint32_t b = 0;
       if (k < K && key < nkeys) {
@@ -732,23 +750,21 @@ __global__ void __launch_bounds__(256) k_dec_coef0_tiled(const uint32_t *__restr
           b = t == 0 ? (sk[0] ? q - sk[0] : 0u) : sk[n - t];
         }
       }
-      Bs[c0_swz_b(kk, j)] = b;
+      Bs[c0_swz<TN, RJ>(kk, j)] = b;
     }
     __syncthreads();
 #pragma unroll 2
     for (int kk = 0; kk < kC0Kc; kk += 4) {
-      uint32_t a[4][4], b[4][2];
+      uint32_t a[4][RI], b[4][RJ];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const uint4 av = *reinterpret_cast<const uint4 *>(&As[c0_swz_a(kk + u, ty * 4)]);
-        const uint2 bv = *reinterpret_cast<const uint2 *>(&Bs[c0_swz_b(kk + u, tx * 2)]);
-        a[u][0] = av.x, a[u][1] = av.y, a[u][2] = av.z, a[u][3] = av.w;
-        b[u][0] = bv.x, b[u][1] = bv.y;
+        c0_row<RI>(&As[c0_swz<TM, RI>(kk + u, ty * RI)], a[u]);
+        c0_row<RJ>(&Bs[c0_swz<TN, RJ>(kk + u, tx * RJ)], b[u]);
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < RI; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < RJ; ++j) {
           uint64_t t = (uint64_t)a[0][i] * b[0][j];
 #pragma unroll
           for (int u = 1; u < 4; ++u) t += (uint64_t)a[u][i] * b[u][j];
@@ -761,11 +777,11 @@ __global__ void __launch_bounds__(256) k_dec_coef0_tiled(const uint32_t *__restr
   }
   const uint64_t c64 = 0ull - mu * q;  // 2^64 mod q
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int c = ct0 + ty * 4 + i;
+  for (int i = 0; i < RI; ++i) {
+    const int c = ct0 + ty * RI + i;
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int key = key0 + tx * 2 + j;
+    for (int j = 0; j < RJ; ++j) {
+      const int key = key0 + tx * RJ + j;
       if (c < nct && key < nkeys)
         d0[((size_t)c * nkeys + key) * 3 + m] = mod_u64(mod_u64(lo[i][j], mu, q) + (uint64_t)hi[i][j] * c64, mu, q);
     }
@@ -1041,7 +1057,15 @@ static int encrypt_tail(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *
     constexpr int G = ppc<LOGN>(), NT = NttPlan<LOGN>::T * G;
     constexpr int MINB = NT >= 1024 ? 1 : 1024 / NT;  // 64 registers
     ProfScope ps("encrypt_intt", s);
-    if (batch >= 2) {  // two instances per thread group
+    // instances per thread group: the tuner's choice for this batch size, else two from batch 2
+    int group = batch >= 2 ? 2 : 1;
+    if (c.enc_group_forced) {
+      group = c.enc_group_forced;
+    } else {
+      const auto it = c.enc_group.find(batch);
+      if (it != c.enc_group.end()) group = it->second;
+    }
+    if (group == 2 && batch >= 2) {  // two instances per thread group
       auto kern = k_encrypt<LOGN, 2, MINB>;
       const long long nw = (long long)(c.l + 1) * 3 * ((batch + 1) / 2);
       CUFE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -1311,10 +1335,24 @@ int ctx_decode(Ctx &c, int count, const uint32_t *d_dy, int ncoeff, uint32_t *d_
   return CUFE_OK;
 }
 
-int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
-                      const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s) {
-  if (nct < 1 || nkeys < 1 || (long long)nct * nkeys > 0x7fffffffLL || !d_out) return CUFE_ERR_INVALID;
-  if (nkeys < kCoef0TiledMinKeys) {
+// the tiled product with RI x RJ pairs per thread
+template <int RI, int RJ>
+static int launch_coef0_tiled(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                              const uint32_t *d_sky, uint32_t *d0, cudaStream_t s) {
+  const dim3 grid((unsigned)((nct + 16 * RI - 1) / (16 * RI)), (unsigned)((nkeys + 16 * RJ - 1) / (16 * RJ)), 3);
+  note_launch(), k_dec_coef0_tiled<RI, RJ><<<grid, 256, 0, s>>>(d_ct, d_y, y_signed, nct, nkeys, d_sky, d0,
+                                                                  scheme_args(c));
+  CUFE_CUDA(cudaGetLastError());
+  return CUFE_OK;
+}
+
+// form 0: one CTA per (ciphertext, key) pair; 1..4: the tiled product at 64x32, 64x64, 32x32,
+// 32x64 (ciphertexts x keys) then the decode of every pair
+int ctx_decrypt_coef0_form(Ctx &c, int form, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y,
+                           int y_signed, const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s) {
+  if (nct < 1 || nkeys < 1 || (long long)nct * nkeys > 0x7fffffffLL || !d_out || form < 0 || form >= kCoef0Forms)
+    return CUFE_ERR_INVALID;
+  if (form == 0) {
     ProfScope ps("decrypt_coef0", s);
     note_launch(), k_dec_coef0<<<(unsigned)(nct * nkeys), 256, 0, s>>>(d_ct, d_y, y_signed, nkeys, d_sky, d_d0, d_out,
                                                         scheme_args(c), decode_args(c));
@@ -1330,12 +1368,88 @@ int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const ui
     d0 = reinterpret_cast<uint32_t *>(c.ws);
   }
   ProfScope ps("decrypt_coef0", s);
-  const dim3 grid((unsigned)((nct + kC0Tm - 1) / kC0Tm), (unsigned)((nkeys + kC0Tn - 1) / kC0Tn), 3);
-  note_launch(), k_dec_coef0_tiled<<<grid, 256, 0, s>>>(d_ct, d_y, y_signed, nct, nkeys, d_sky, d0, scheme_args(c));
-  CUFE_CUDA(cudaGetLastError());
+  int rc = CUFE_OK;
+  if (form == 1) rc = launch_coef0_tiled<4, 2>(c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d0, s);
+  if (form == 2) rc = launch_coef0_tiled<4, 4>(c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d0, s);
+  if (form == 3) rc = launch_coef0_tiled<2, 2>(c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d0, s);
+  if (form == 4) rc = launch_coef0_tiled<2, 4>(c, nct, d_ct, nkeys, d_y, y_signed, d_sky, d0, s);
+  if (rc) return rc;
   note_launch(), k_decode_triples<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(d0, npairs, d_out, decode_args(c));
   CUFE_CUDA(cudaGetLastError());
   return CUFE_OK;
+}
+
+// device time of one call of f() on s after one untimed call (the better of two timed calls)
+template <class F>
+static int time_call(F f, cudaStream_t s, float *ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUFE_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    set_last_error("tuner: cudaEventCreate failed");
+    return CUFE_ERR_CUDA;
+  }
+  int rc = f();
+  float best = 0;
+  for (int rep = 0; rep < 2 && rc == CUFE_OK; ++rep) {
+    float t = 0;
+    if (cudaEventRecord(e0, s) != cudaSuccess || (rc = f()) != CUFE_OK) break;
+    if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+      set_last_error("tuner: event timing failed");
+      rc = CUFE_ERR_CUDA;
+      break;
+    }
+    best = rep == 0 ? t : std::min(best, t);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = best;
+  return rc;
+}
+
+int ctx_tune_encrypt(Ctx &c, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                     const uint8_t *seeds3, uint32_t *d_ct, int *choice, float *ms, cudaStream_t s) {
+  if (batch < 1 || !seeds2) return CUFE_ERR_INVALID;
+  float t[2] = {0, 0};
+  int rc = CUFE_OK;
+  for (int g = 1; g <= 2 && rc == CUFE_OK; ++g) {
+    c.enc_group_forced = g;
+    rc = time_call([&] { return ctx_encrypt_cpu_map(c, batch, d_x, d_mpk, seeds2, seeds3, d_ct, s); }, s, &t[g - 1]);
+  }
+  c.enc_group_forced = 0;
+  if (rc) return rc;
+  const int best = (batch >= 2 && t[1] < t[0]) ? 2 : 1;
+  c.enc_group[batch] = best;
+  if (choice) *choice = best;
+  if (ms) ms[0] = t[0], ms[1] = t[1];
+  return CUFE_OK;
+}
+
+int ctx_tune_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                           const uint32_t *d_sky, uint32_t *d_out, int *choice, float *ms, cudaStream_t s) {
+  if (nct < 1 || nkeys < 1 || !d_out) return CUFE_ERR_INVALID;
+  float t[kCoef0Forms] = {};
+  int best = 0;
+  for (int f = 0; f < kCoef0Forms; ++f) {
+    const int rc = time_call(
+        [&] { return ctx_decrypt_coef0_form(c, f, nct, d_ct, nkeys, d_y, y_signed, d_sky, nullptr, d_out, s); }, s,
+        &t[f]);
+    if (rc) return rc;
+    if (t[f] < t[best]) best = f;
+  }
+  c.coef0_form[{nct, nkeys}] = best;
+  if (choice) *choice = best;
+  if (ms)
+    for (int f = 0; f < kCoef0Forms; ++f) ms[f] = t[f];
+  return CUFE_OK;
+}
+
+int ctx_decrypt_coef0(Ctx &c, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                      const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, cudaStream_t s) {
+  const auto it = c.coef0_form.find({nct, nkeys});
+  const int form = it != c.coef0_form.end() ? it->second : (nkeys < kCoef0TiledMinKeys ? 0 : 1);
+  return ctx_decrypt_coef0_form(c, form, nct, d_ct, nkeys, d_y, y_signed, d_sky, d_d0, d_out, s);
 }
 
 int ctx_sample_cpu_map(Ctx &c, int sig, int nstreams, const uint8_t *keys, int calls, uint32_t *d_out,

@@ -142,17 +142,32 @@ int svm_create(Ctx &c, SvmModel &m, int nr_class, int lsv, const int32_t *sv, in
   return CUFE_OK;
 }
 
+// the model's kvalue scratch for nct test vectors
+static int kval_scratch(SvmModel &m, int nct) {
+  if (nct > m.cap) {
+    if (m.d_kval) CUFE_CUDA(cudaFree(m.d_kval));
+    m.d_kval = nullptr;
+    CUFE_CUDA(cudaMalloc(&m.d_kval, (size_t)nct * m.lsv * 4));
+    m.cap = nct;
+  }
+  return CUFE_OK;
+}
+
+// the coefficient-0 decrypt form for nct test vectors against the model's support vectors
+int svm_tune(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *choice, float *ms, cudaStream_t s) {
+  if (nct < 1 || !d_ct) return CUFE_ERR_INVALID;
+  const int rc = kval_scratch(m, nct);
+  if (rc) return rc;
+  return ctx_tune_decrypt_coef0(c, nct, d_ct, m.lsv, m.d_y, m.y_signed, m.d_sky, m.d_kval, choice, ms, s);
+}
+
 int svm_predict(Ctx &c, SvmModel &m, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kval, double *d_dec,
                 cudaStream_t s) {
   if (nct < 1 || !d_ct || !d_label) return CUFE_ERR_INVALID;
   uint32_t *kv = d_kval;
   if (!kv) {
-    if (nct > m.cap) {
-      if (m.d_kval) CUFE_CUDA(cudaFree(m.d_kval));
-      m.d_kval = nullptr;
-      CUFE_CUDA(cudaMalloc(&m.d_kval, (size_t)nct * m.lsv * 4));
-      m.cap = nct;
-    }
+    const int rc = kval_scratch(m, nct);
+    if (rc) return rc;
     kv = m.d_kval;
   }
   int rc = ctx_decrypt_coef0(c, nct, d_ct, m.lsv, m.d_y, m.y_signed, m.d_sky, nullptr, kv, s);

@@ -149,6 +149,23 @@ int cufe_decode(cufe_ctx *ctx, int count, const uint32_t *d_dy, int ncoeff, uint
 int cufe_decrypt_coef0(cufe_ctx *ctx, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
                        const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, void *stream);
 
+/* Shape tuners (no counterpart in the reference, which has one fixed launch shape per kernel).
+ * Each times every form of one operation on the caller's buffers -- all forms give the same
+ * bits, so the outputs are valid whichever ran last -- and keeps the fastest on the context
+ * for that shape; later calls of the same shape use it (other shapes keep the fixed rules).
+ *   cufe_tune_encrypt: one or two instances per thread group in the encryption kernel, for this
+ *     batch size (fixed rule: two from batch 2); choice = 1 or 2, ms[2];
+ *   cufe_tune_decrypt_coef0: for (nct, nkeys), form 0 = one CTA per (ciphertext, key) pair, 1..4
+ *     = the tiled product at 64x32, 64x64, 32x32, 32x64 ciphertexts x keys per CTA (fixed rule:
+ *     form 0 below 32 keys, else 1); choice = the form, ms[5];
+ *   cufe_decrypt_coef0_form: cufe_decrypt_coef0 in the given form (tests, comparisons). */
+int cufe_tune_encrypt(cufe_ctx *ctx, int batch, const uint32_t *d_x, const uint32_t *d_mpk, const uint8_t *seeds2,
+                      const uint8_t *seeds3, uint32_t *d_ct, int *choice, float *ms, void *stream);
+int cufe_tune_decrypt_coef0(cufe_ctx *ctx, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y, int y_signed,
+                            const uint32_t *d_sky, uint32_t *d_out, int *choice, float *ms, void *stream);
+int cufe_decrypt_coef0_form(cufe_ctx *ctx, int form, int nct, const uint32_t *d_ct, int nkeys, const uint32_t *d_y,
+                            int y_signed, const uint32_t *d_sky, uint32_t *d_d0, uint32_t *d_out, void *stream);
+
 /* samplers, for parity tests and statistics.  CPU mapping: nstreams AES-CTR streams keyed by
  * keys[nstreams][32] (NULL: zero-key streams), each running `calls` consecutive
  * gaussian_sampler_S* calls of n samples (src/gauss.c:789,995,1086): d_out[nstreams][calls][3][n]. */
@@ -213,6 +230,9 @@ int cufe_svm_create(cufe_svm **svm, cufe_ctx *ctx, int nr_class, int nsv_total, 
  * [nct][nsv_total] and d_dec [nct][pairs] are optional (device, NULL to skip). */
 int cufe_svm_predict(cufe_svm *svm, int nct, const uint32_t *d_ct, int *d_label, uint32_t *d_kvalue, double *d_dec,
                      void *stream);
+/* the coefficient-0 decrypt form for nct ciphertexts against the model's support vectors
+ * (cufe_tune_decrypt_coef0 on the model's keys); choice and ms[5] as there */
+int cufe_svm_tune(cufe_svm *svm, int nct, const uint32_t *d_ct, int *choice, float *ms, void *stream);
 int cufe_svm_destroy(cufe_svm *svm);
 
 /* =====================================================================================
@@ -247,6 +267,10 @@ int cufe_batch_run(cufe_batch *batch, void *stream);
  * that call if none ran) and replayed afterwards: the graph reads the bound buffers' current
  * contents, so new seeds or inputs written there take effect on the next replay */
 int cufe_batch_replay(cufe_batch *batch, void *stream);
+/* Re-lays the chunks of a bound batch for each scratch budget budgets[0..ncand-1] (keys stay
+ * resident), times one eager step each and keeps the fastest layout; ms[i] = -1 for a budget
+ * whose scratch does not fit the device.  No counterpart in the reference.  Drops the graph. */
+int cufe_batch_tune(cufe_batch *batch, int ncand, const size_t *budgets, size_t *chosen, float *ms, void *stream);
 /* kernel timing of eager steps (cufe_batch_run): on != 0 clears and starts it; read gives the
  * summed device milliseconds of the step's kernel groups (CUDA events around each group on the
  * step's stream) and the number of kernels launched; with it the cost of the graph's launch
