@@ -103,9 +103,9 @@ void modeb_prepare_key(const unsigned char seed[32], unsigned char rk[240]) {
 }
 
 /* one block of the sigma_{sig+1} kernel keyed by the 32-byte seed: out[3][SIFE_N] = the residues
- * of polynomial `bid` (0 <= bid < 64).  Returns 0, or a negative value if the scheduler failed. */
+ * of polynomial `bid` (0 <= bid < 4096).  Returns 0, or a negative value if the scheduler failed. */
 int modeb_block(int sig, const unsigned char seed[32], int bid, uint32_t *out) {
-  if (sig < 0 || sig > 2 || bid < 0 || bid >= 64) return -3;
+  if (sig < 0 || sig > 2 || bid < 0 || bid >= 4096) return -3;
   static unsigned char rk[240];
   modeb_prepare_key(seed, rk);
   const size_t poly = (size_t)SIFE_NMODULI * SIFE_N;

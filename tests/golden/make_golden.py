@@ -28,6 +28,12 @@ Outputs:
                     and 6 support vectors (the vote's term loops at odd and even short
                     lengths), written in libsvm's format and read by the reference's own
                     svm_load_model, 12 test vectors
+  ref_modeb_setup.json  the drop-in setup at the reference's own shape (n = 4096, l = 785):
+                    SHA-256 of msk and mpk when s_i and e_i come from the reference's S1 GPU
+                    kernel run on the host (blocks 0..784, keys seed2 and seed3, as
+                    src/rlwe_sife_gpu.cu:61-62 launches it), a from the reference CPU
+                    sample_polya(seed1), and mpk_i = NTT(a) NTT(s_i) + NTT(e_i) with the
+                    reference CPU NTT (src/rlwe_sife_gpu.cu:64-71)
   ref_modeb.npz     the GPU counter-to-sample mapping (mode B) from the reference's own kernel
                     bodies (src/sample_gpu.cu) run on the host by oracle/_ref/modeb/libmodeb.so:
                     polynomial 0 (the first 4096 samples) per sigma for two keys as signed
@@ -184,6 +190,34 @@ def svm_small():
                         ref_kvalue=np.array(kvs).astype(np.uint16))
 
 
+def _modeb_block(args):
+    sig, seed, bid = args
+    return canon(ReferenceModeB().poly(sig, seed, bid))
+
+
+def modeb_setup():
+    import multiprocessing as mp
+    R = Reference("default")
+    n, l = R.n, R.l
+    seed1, seed2, seed3 = np.random.default_rng(0xC0FE0202).integers(0, 256, (3, 32), dtype=np.uint8)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        s = np.stack(pool.map(_modeb_block, [(0, seed2, i) for i in range(l)], chunksize=8))
+        e = np.stack(pool.map(_modeb_block, [(0, seed3, i) for i in range(l)], chunksize=8))
+    q = np.array(Q, np.uint64)[:, None]
+    a = R.sample_polya(seed1)
+    a_hat = np.stack([R.ntt(a[j], j) for j in range(3)]).astype(np.uint64) % q
+    mpk = np.zeros((l + 1, 3, n), np.uint32)
+    for i in range(l):
+        s_hat = np.stack([R.ntt(s[i][j], j) for j in range(3)]).astype(np.uint64) % q
+        e_hat = np.stack([R.ntt(e[i][j], j) for j in range(3)]).astype(np.uint64) % q
+        mpk[i] = ((a_hat * s_hat % q + e_hat) % q).astype(np.uint32)
+    mpk[l] = a_hat.astype(np.uint32)
+    doc = {"n": n, "l": l, "seed1": seed1.tolist(), "seed2": seed2.tolist(), "seed3": seed3.tolist(),
+           "a_sha": sha(canon(a)), "msk_sha": sha(s), "mpk_sha": sha(mpk)}
+    with open(os.path.join(HERE, "ref_modeb_setup.json"), "w") as f:
+        json.dump(doc, f, indent=1)
+
+
 def _svm_init(model_path, seed_a, seed_e):
     global _R, _M, _MSK, _MPK
     _R = ReferenceCallers()
@@ -237,6 +271,7 @@ if __name__ == "__main__":
     small()
     c2()
     modeb()
+    modeb_setup()
     svm(root)
     svm_small()
     print("golden fixtures written to", HERE)

@@ -383,6 +383,27 @@ def test_dropin_abi(rng, oracle_built):
         assert int(O.decode(rdy)[0]) == int(x[0].astype(np.int64) @ y[k].astype(np.int64))
 
 
+def test_dropin_setup_at_the_reference_shape(oracle_built):
+    """rlwe_sife_setup_gpu at the reference's compile-time shape (n 4096, l 785, the default
+    configuration) against tests/golden/ref_modeb_setup.json, made from the reference's own S1
+    GPU kernel (run on the host), CPU sample_polya and CPU NTT"""
+    import ctypes as C
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_modeb_setup.json")))
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    n, l = d["n"], d["l"]
+    L = cf.lib()
+    assert L.cufe_dropin_configure(n, l, 0) == 0
+    mpk = np.zeros((l + 1, 3, n), np.uint32)
+    msk = np.zeros((l, 3, n), np.uint32)
+    mpk[l] = Oracle(n, 1).sample_polya(np.array(d["seed1"], np.uint8))
+    assert sha(canon(mpk[l])) == d["a_sha"]
+    s2, s3 = np.array(d["seed2"], np.uint8), np.array(d["seed3"], np.uint8)
+    t = C.c_float(0)
+    L.rlwe_sife_setup_gpu(mpk.ctypes.data, msk.ctypes.data, s2.ctypes.data, s3.ctypes.data, C.byref(t))
+    assert L.cufe_dropin_status() == 0
+    assert sha(msk) == d["msk_sha"] and sha(mpk) == d["mpk_sha"]
+
+
 def test_dropin_staged_copies(rng, oracle_built):
     """the drop-in symbols at sizes that take the pinned, chunked host copies (mpk and msk
     of 9.8 MB, two ciphertexts of 19.7 MB: ragged last chunks), against the context API on

@@ -125,6 +125,20 @@ def test_modeb_golden(oracle_built):
                 assert sha(canon(O.gauss_modeB(rk, sig, bid))) == hashes["k%d_s%d_b%d" % (k, sig, bid)], (k, sig, bid)
 
 
+@pytest.mark.slow
+def test_modeb_setup_reference_shape(oracle_built):
+    """setup in the GPU counter mapping at the reference's own shape (n 4096, l 785) against
+    tests/golden/ref_modeb_setup.json: s_i, e_i from the reference's S1 GPU kernel run on the
+    host, a from its CPU sample_polya, mpk through its CPU NTT"""
+    d = json.load(open(os.path.join(GOLD, "ref_modeb_setup.json")))
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()  # noqa: E731
+    O = Oracle(d["n"], d["l"])
+    a = O.sample_polya(np.array(d["seed1"], np.uint8))
+    assert sha(canon(a)) == d["a_sha"]
+    mpk, msk = O.setup_modeB(a, np.array(d["seed2"], np.uint8), np.array(d["seed3"], np.uint8))
+    assert sha(canon(msk)) == d["msk_sha"] and sha(canon(mpk)) == d["mpk_sha"]
+
+
 def _have_modeb():
     return os.path.exists(os.path.join(os.path.dirname(GOLD), "..", "oracle", "_ref", "modeb", "libmodeb.so"))
 
