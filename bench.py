@@ -456,11 +456,11 @@ def gpu_arm(args):
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
 
     def lds_pipe(batch, launch_s):
-        # the AES keystream bounds the sigma_3 candidate kernel: 14 AES-256 blocks per refill;
+        # the AES keystream bounds the sigma_3 candidate kernel: 13 AES-256 blocks per refill;
         # with the counter caching a block takes 1 + 4 + 11 x 16 + 16 = 197 T-table lookups from
         # shared memory, plus 15 per refill for the round-2 constants (one warp LDS per clock
         # per SM): 198 per block
-        blocks = refills3 * batch * 14
+        blocks = refills3 * batch * 13
         lds_peak = 148 * sm_mhz * 1e6 * 32 / 198
         return {"what": "AES-256 blocks/s (T-table, shared-memory LDS bound)", "achieved": blocks / launch_s,
                 "peak_lds_bound": lds_peak, "frac": blocks / launch_s / lds_peak, "sm_mhz": sm_mhz}
@@ -511,7 +511,7 @@ def gpu_arm(args):
         line["c4_ntt"] = ntt_point(4096, 3, 65536, 10, 3)
         mixed = mixed_measure(4096, 5, 3, 24)
         line["c3_batched"] = {k: mixed[k] for k in ("value", "unit", "ms_per_step", "p50_ms", "p99_ms", "bit_exact",
-                                                    "setup_s", "graph", "sigma3_samples_per_s")}
+                                                    "setup_s", "graph", "sigma3_samples_per_s", "kernels_ms")}
         line["c3_batched"]["config"] = mixed["config"]
         serve = serve_measure(64, [5000, 10000, 20000, 50000], 0.5, 48, 24, 30,
                               max_tick=args.serve_max_tick, max_queue_s=args.serve_max_queue_ms / 1000.0)
@@ -818,6 +818,7 @@ def mixed_measure(count, steps, warmup, chunk_gb, tune_gb=(12, 24, 36)):
     res[steps].copy_(out)
     torch.cuda.synchronize()
     kernel_ms, kernels = B.profile_read()
+    groups = B.profile_groups()
     B.profile(False)
     eager_ms = g0.elapsed_time(g1)
     p = np.array([64 * l + 1 for l in ls], np.int64)
@@ -835,6 +836,7 @@ def mixed_measure(count, steps, warmup, chunk_gb, tune_gb=(12, 24, 36)):
                       "eager_kernel_ms": kernel_ms, "eager_kernels": kernels, "eager_step_ms": eager_ms,
                       "replay_over_kernel_time": replay_ms / kernel_ms if kernel_ms else None,
                       "note": "kernel time from CUDA events around every kernel group of one eager step"},
+            "kernels_ms": {k: {"launches": v[0], "ms": v[1]} for k, v in sorted(groups.items(), key=lambda kv: -kv[1][1])},
             "config": {"workload": "%d instances, l log-uniform [32, 1024], N 2048/4096 50/50, one CUDA graph "
                                    "replay per step" % count,
                        "instances": count, "mean_l": float(np.mean(ls)), "n4096_share": float(np.mean(np.array(ns) == 4096)),

@@ -92,6 +92,7 @@ def lib():
             "cufe_batch_profile": [vp, i],
             "cufe_batch_profile_read": [vp, vp, vp],
             "cufe_batch_graph_kernels": [vp],
+            "cufe_batch_profile_groups": [vp, i, vp, vp, vp],
             "cufe_svm_create": [C.POINTER(vp), vp, i, i, vp, i, vp, vp, vp, vp, vp, vp],
             "cufe_svm_predict": [vp, i, vp, vp, vp, vp, vp],
             "cufe_svm_destroy": [vp],
@@ -561,6 +562,16 @@ class Batch:
         ms, k = C.c_double(0), C.c_longlong(0)
         _check(lib().cufe_batch_profile_read(self.h, C.byref(ms), C.byref(k)), "cufe_batch_profile_read")
         return ms.value, k.value
+
+    def profile_groups(self):
+        """{group name: (kernels launched, ms)} of the profiled eager steps"""
+        names = C.create_string_buffer(64 * 64)
+        launches = (C.c_longlong * 64)()
+        ms = (C.c_double * 64)()
+        k = lib().cufe_batch_profile_groups(self.h, 64, names, launches, ms)
+        if k < 0:
+            raise CufeError(k, "cufe_batch_profile_groups")
+        return {names.raw[64 * i:64 * i + 64].split(b"\0")[0].decode(): (launches[i], ms[i]) for i in range(k)}
 
     def graph_kernels(self):
         r = lib().cufe_batch_graph_kernels(self.h)

@@ -1273,6 +1273,24 @@ int cufe_batch_profile_read(cufe_batch *h, double *kernel_ms, long long *kernels
   return CUFE_OK;
 }
 
+int cufe_batch_profile_groups(cufe_batch *h, int max_groups, char *names, long long *launches, double *ms) {
+  if (!h) return CUFE_ERR_INVALID;
+  std::lock_guard<std::mutex> g(h->mu);
+  h->prof.collect();
+  int i = 0;
+  for (const auto &kv : h->prof.acc) {
+    if (i >= max_groups) break;
+    if (names) {
+      std::strncpy(names + 64 * (size_t)i, kv.first.c_str(), 63);
+      names[64 * (size_t)i + 63] = 0;
+    }
+    if (launches) launches[i] = kv.second.first;
+    if (ms) ms[i] = kv.second.second;
+    ++i;
+  }
+  return i;
+}
+
 int cufe_batch_graph_kernels(cufe_batch *h) {
   if (!h) return CUFE_ERR_INVALID;
   std::lock_guard<std::mutex> g(h->mu);

@@ -39,9 +39,10 @@ __device__ __noinline__ void ctr_block_g(uint32_t (&W)[4], uint32_t ctr, const u
   aes256_ctr_block(W, 0u, ctr, rk, c);
 }
 
-// uniform draws when the first 12 words hold fewer than 8 accepted ones (probability below
-// 1e-7 per refill): rescan bytes 200.. with the rejection loop of src/gauss.c:578-703,
-// regenerating blocks as needed
+// uniform draws when the first 10 words hold fewer than 8 accepted ones (at least 3 of 10
+// draws rejected: about 7e-5 per refill for sigma_2 and sigma_3, whose rejection rate is
+// 1 - 7 K / 2^32 = 0.84%; far less for sigma_1): rescan bytes 200.. with the rejection loop of
+// src/gauss.c:578-703, regenerating blocks as needed
 template <int SIG>
 __device__ __noinline__ void uniform_slow(uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
                                           const AesCtx &c, uint32_t *status) {
@@ -95,19 +96,20 @@ __device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb,
 // Blocks of one refill that the fast path reads (16-byte block b = bytes 16b..16b+15, word w
 // = bytes 4w..4w+3): 2, 3 (CDT high words of lanes 0..3, words 8..15), 4, 5, 6 (Bernoulli
 // words 16..24), 8..12 (CDT high words and Bernoulli words of lanes 4..7, words 33..49),
-// 12..15 (the first 12 uniform words from byte 200, words 50..61) and 17 (sign byte 280,
-// word 70).  Blocks 0, 1, 7 hold only the low CDT words, which S1/S2 never use and S3 uses
-// only on ties; block 16 holds uniform words 64..67, needed only when fewer than 8 of the
-// first 12 words are accepted.  Both rare cases regenerate what they need on their slow
-// paths.  Buffer word kbuf(w) holds refill word w.
-constexpr int kRefillBlocks = 14;
-__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 15, 17};
-__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : (w < 64 ? w - 12 : w - 16); }
-static_assert(kbuf(70) == 4 * 13 + 2, "sign word lives in block 17, the last buffer block");
-static_assert(kbuf(61) == 4 * 12 + 1, "uniform words end in block 15");
+// 12..14 (the first 10 uniform words from byte 200, words 50..59) and 17 (sign byte 280,
+// word 70): 13 of the refill's 24 blocks.  Blocks 0, 1, 7 hold only the low CDT words, which
+// S1/S2 never use and S3 uses only on ties; blocks 15 and 16 hold uniform words 60..67, needed
+// only when fewer than 8 of the first 10 words are accepted.  Both rare cases regenerate what
+// they need on their slow paths.  Buffer word kbuf(w) holds refill word w.
+constexpr int kRefillBlocks = 13;
+__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 17};
+__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : (w < 60 ? w - 12 : w - 20); }
+static_assert(kbuf(70) == 4 * 12 + 2, "sign word lives in block 17, the last buffer block");
+static_assert(kbuf(59) == 4 * 11 + 3, "uniform words end in block 14");
+static_assert(kbuf(49) == 4 * 9 + 1 && kbuf(50) == 4 * 9 + 2, "block 12 holds words 48..51");
 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
-constexpr int kUniformWords = 12;  // words scanned branch-free; more are needed with p < 1e-7
+constexpr int kUniformWords = 10;  // words scanned branch-free (blocks 12..14); more with p ~ 7e-5
 
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)

@@ -277,6 +277,9 @@ int cufe_batch_tune(cufe_batch *batch, int ncand, const size_t *budgets, size_t 
  * gaps is replay time / kernel time.  No counterpart in the reference. */
 int cufe_batch_profile(cufe_batch *batch, int on);
 int cufe_batch_profile_read(cufe_batch *batch, double *kernel_ms, long long *kernels);
+/* the same per named kernel group (64-byte name slots), as cufe_profile_read; returns the
+ * number of groups written */
+int cufe_batch_profile_groups(cufe_batch *batch, int max_groups, char *names, long long *launches, double *ms);
 /* kernel nodes of the captured step graph (0 before the first replay) */
 int cufe_batch_graph_kernels(cufe_batch *batch);
 /* synchronous check of the batch's sampler status word (CUFE_ERR_SAMPLER if set) */
