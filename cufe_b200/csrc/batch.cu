@@ -477,8 +477,11 @@ int Batch::tune(int nb, const size_t *budgets, size_t *chosen, float *ms, cudaSt
     if (rc == CUFE_ERR_NOMEM) continue;
     if (rc) return rc;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    CUFE_CUDA(cudaEventCreate(&e0));
-    CUFE_CUDA(cudaEventCreate(&e1));
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      if (e0) cudaEventDestroy(e0);
+      set_last_error("batch tune: cudaEventCreate failed");
+      return CUFE_ERR_CUDA;
+    }
     float t = 0;
     rc = run(s);  // untimed: first use of this layout
     if (!rc && cudaEventRecord(e0, s) == cudaSuccess) rc = run(s);
@@ -540,6 +543,10 @@ int Batch::run(cudaStream_t s) {
   if (!x || !y || !seeds2 || !seeds3 || !out) {
     set_last_error("batch: bind the inputs and outputs first");
     return CUFE_ERR_INVALID;
+  }
+  if (!scratch || !tables) {  // a re-layout (cufe_batch_tune) that found no memory
+    set_last_error("batch: no step scratch; re-chunk with a budget that fits");
+    return CUFE_ERR_NOMEM;
   }
   uint32_t *rk2 = rk, *rk3 = rk + (size_t)count * 60;
   int rc = expand_keys_device(seeds2, perm, count, rk2, s);
