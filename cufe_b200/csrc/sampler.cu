@@ -344,26 +344,31 @@ __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__re
   uint32_t a = 0;
   bool bad = v.R == 0;
   uint32_t c = 0;
+  // exclusive prefix at a, the start of the current call; afterwards it is carried over from
+  // the search, where the lane that found a call's last refill e has read prefix_at(e + 1)
+  uint32_t base = bad ? 0u : prefix_at(elocal, tile_off, amask, v, 0);
   for (; c < calls && !bad; ++c) {
-    const uint32_t base = prefix_at(elocal, tile_off, amask, v, a);
     const uint32_t target = base + n;
     // smallest e >= a whose inclusive prefix reaches target (monotone in e), searched in
     // windows of 32 refills around the expected call length; `known` is a position already
-    // seen to satisfy.  Upward moves stop at the refill range, downward moves at a.
+    // seen to satisfy (its prefix in known_pv).  Upward moves stop at the refill range,
+    // downward moves at a.
     uint32_t lo = a + (guess > 16 ? guess - 16 : 0);
     int64_t known = -1;
-    uint32_t e = 0;
+    uint32_t known_pv = 0, e = 0, next_base = 0;
     for (int it = 0;; ++it) {
       if (it > (1 << 22)) {  // cannot happen for a monotone prefix; bounded regardless
         bad = true;
         break;
       }
       const uint32_t j = lo + lane;
-      const bool ok = (j < v.R) && prefix_at(elocal, tile_off, amask, v, j + 1) >= target;
+      const uint32_t pv = j < v.R ? prefix_at(elocal, tile_off, amask, v, j + 1) : 0u;
+      const bool ok = (j < v.R) && pv >= target;
       const uint32_t bal = __ballot_sync(0xffffffffu, ok);
       if (bal == 0) {
         if (known >= 0) {
           e = (uint32_t)known;
+          next_base = known_pv;
           break;
         }
         if (lo + 32 >= v.R) {
@@ -374,16 +379,20 @@ __global__ void k_walk(const uint32_t *__restrict__ elocal, const uint32_t *__re
         continue;
       }
       const int first = __ffs(bal) - 1;
+      const uint32_t first_pv = __shfl_sync(0xffffffffu, pv, first);
       if (first > 0 || lo == a) {
         e = lo + first;
+        next_base = first_pv;
         break;
       }
       known = lo;
+      known_pv = first_pv;
       lo = lo > a + 32 ? lo - 32 : a;
     }
     if (bad) break;
     if (lane == 0) cs[c] = a;
     a = e + 1;
+    base = next_base;
   }
   if (lane == 0) {
     if (bad) atomicOr(status, kStatusRefillsExhausted);
