@@ -22,19 +22,25 @@ def _stale():
 
 
 def build(force=False, verbose=False):
+    """compile every source (in parallel, one nvcc per file) and link the shared library;
+    without force only when a source or the public header is newer than the library"""
+    from concurrent.futures import ThreadPoolExecutor
     if not force and not _stale():
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
     extra = ["-Xptxas", "-v"] if verbose else []
-    for src in SOURCES:
+
+    def compile_one(src):
         obj = os.path.join(objdir, src + ".o")
         cmd = [NVCC, "-c", os.path.join(CSRC, src), "-o", obj] + FLAGS + extra
         if src.endswith(".cpp"):
             cmd += ["-x", "cu"]
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, "-shared", "-o", tmp] + objs + ["-gencode", "arch=compute_100a,code=sm_100a"],
                    check=True)

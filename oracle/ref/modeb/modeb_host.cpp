@@ -60,7 +60,8 @@ void thread_main() {
 
 /* run every thread of block `bid` to completion, barrier generation by generation */
 int run_block(unsigned bid, unsigned nthreads) {
-  std::vector<std::vector<char>> stacks(nthreads, std::vector<char>(kStack));
+  static std::vector<std::vector<char>> stacks;  // reused across blocks
+  if (stacks.size() < nthreads) stacks.resize(nthreads, std::vector<char>(kStack));
   g_ctx.assign(nthreads, ucontext_t{});
   g_done.assign(nthreads, 0);
   blockIdx = {bid, 0, 0};
