@@ -157,7 +157,9 @@ def build_modeb(root, force=False):
     device headers compiled as host C++ by oracle/ref/modeb/modeb_host.cpp"""
     d = os.path.join(OUT, "modeb")
     lib = os.path.join(d, "libmodeb.so")
-    if os.path.exists(lib) and not force:
+    shim = os.path.join(HERE, "modeb")
+    newest = max(os.path.getmtime(os.path.join(shim, f)) for f in os.listdir(shim))
+    if os.path.exists(lib) and not force and os.path.getmtime(lib) >= newest:
         return lib
     os.makedirs(d, exist_ok=True)
     src_dir = os.path.join(root, "src")
@@ -168,7 +170,6 @@ def build_modeb(root, force=False):
                 "not committed */\n")
         for body in extract_functions(text, MODEB_FUNCS):
             f.write(body + "\n\n")
-    shim = os.path.join(HERE, "modeb")
     cmd = (["g++"] + MODEB_FLAGS + ["-I", shim, "-I", src_dir, "-I", d, "-o", lib,
                                     os.path.join(shim, "modeb_host.cpp")])
     subprocess.run(cmd, check=True)
