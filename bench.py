@@ -207,10 +207,11 @@ def cpu_baseline_sample(x, y, seeds2, setup_seeds, nproc, steps=2):
 # ----------------------------------------------------------------------------- GPU arm
 
 # DRAM bytes per refill of the sigma_3 candidate kernel, from one ncu capture of a batch-16
-# launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.49 MB + 676.2 MB over
-# 16 x 1,103,616 refills); traffic grows with the refill count, so a launch of B streams
-# moves B x refills x this
-CAND_S3_DRAM_BYTES_PER_REFILL = (1.494528e6 + 676.216064e6) / (16 * 1103616)
+# launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.23 MB + 530.3 MB over
+# 16 x 1,044,352 refills: 31.8 B against 35 B algorithmic, because the last tens of MB that
+# the launch writes are still in L2 when it ends); traffic grows with the refill count, so a
+# launch of B streams moves B x refills x this
+CAND_S3_DRAM_BYTES_PER_REFILL = (1.231872e6 + 530.28736e6) / (16 * 1044352)
 
 
 # algorithmic HBM bytes per launch of each kernel at this workload (batch B)

@@ -98,6 +98,9 @@ __device__ __forceinline__ void aes256_rounds(uint32_t &s0, uint32_t &s1, uint32
 // of word 0 and three fixed bytes.  k0..k3: the ctr-independent part of round 1 (per key);
 // c0..c3: the fixed part of round 2 for the upper counter bits `hi` (recomputed when they
 // change).  Per block, rounds 1 and 2 then take 1 + 4 table lookups instead of 32.
+// The round-2 keys rk[8..11] are needed only when `hi` changes (about every 10 refills), so
+// they are read from the key schedule in global memory (rkg) and occupy no registers between
+// blocks.
 struct CtrCache {
   uint32_t k0, k1, k2, k3, c0, c1, c2, c3, hi;
 };
@@ -107,23 +110,27 @@ __device__ __forceinline__ void ctr_cache_key(CtrCache &cc, const uint32_t (&rk)
   cc.k0 = te<0>(c, taddr<3>(c, s0)) ^ te<1>(c, taddr<2>(c, s1)) ^ te<2>(c, taddr<1>(c, s2)) ^ rk[4];
   cc.k1 = te<0>(c, taddr<3>(c, s1)) ^ te<1>(c, taddr<2>(c, s2)) ^ te<3>(c, taddr<0>(c, s0)) ^ rk[5];
   cc.k2 = te<0>(c, taddr<3>(c, s2)) ^ te<2>(c, taddr<1>(c, s0)) ^ te<3>(c, taddr<0>(c, s1)) ^ rk[6];
-  cc.k3 = te<1>(c, taddr<2>(c, s0)) ^ te<2>(c, taddr<1>(c, s1)) ^ te<3>(c, taddr<0>(c, s2)) ^ rk[7];
+  cc.k3 =
+      te<1>(c, taddr<2>(c, s0)) ^ te<2>(c, taddr<1>(c, s1)) ^ te<3>(c, taddr<0>(c, s2)) ^ rk[7];
   cc.hi = 0xffffffffu;  // no counter cached
 }
 
-// the keystream block of counter ctr (nonce 0), output as in aes256_ctr_block
+// the keystream block of counter ctr (nonce 0), output as in aes256_ctr_block; rkg: the same
+// key schedule as rk, in global memory
 __device__ __forceinline__ void aes256_ctr_block_cached(uint32_t (&o)[4], uint32_t ctr, const uint32_t (&rk)[60],
-                                                        const AesCtx &c, CtrCache &cc) {
+                                                        const uint32_t *__restrict__ rkg, const AesCtx &c,
+                                                        CtrCache &cc) {
   const uint32_t w3 = ctr ^ rk[3];
   if ((ctr >> 8) != cc.hi) {
     cc.hi = ctr >> 8;
     const uint32_t u1 = cc.k1 ^ te<2>(c, taddr<1>(c, w3));
     const uint32_t u2 = cc.k2 ^ te<1>(c, taddr<2>(c, w3));
     const uint32_t u3 = cc.k3 ^ te<0>(c, taddr<3>(c, w3));
-    cc.c0 = te<1>(c, taddr<2>(c, u1)) ^ te<2>(c, taddr<1>(c, u2)) ^ te<3>(c, taddr<0>(c, u3)) ^ rk[8];
-    cc.c1 = te<0>(c, taddr<3>(c, u1)) ^ te<1>(c, taddr<2>(c, u2)) ^ te<2>(c, taddr<1>(c, u3)) ^ rk[9];
-    cc.c2 = te<0>(c, taddr<3>(c, u2)) ^ te<1>(c, taddr<2>(c, u3)) ^ te<3>(c, taddr<0>(c, u1)) ^ rk[10];
-    cc.c3 = te<0>(c, taddr<3>(c, u3)) ^ te<2>(c, taddr<1>(c, u1)) ^ te<3>(c, taddr<0>(c, u2)) ^ rk[11];
+    const uint4 k2 = __ldg(reinterpret_cast<const uint4 *>(rkg + 8));
+    cc.c0 = te<1>(c, taddr<2>(c, u1)) ^ te<2>(c, taddr<1>(c, u2)) ^ te<3>(c, taddr<0>(c, u3)) ^ k2.x;
+    cc.c1 = te<0>(c, taddr<3>(c, u1)) ^ te<1>(c, taddr<2>(c, u2)) ^ te<2>(c, taddr<1>(c, u3)) ^ k2.y;
+    cc.c2 = te<0>(c, taddr<3>(c, u2)) ^ te<1>(c, taddr<2>(c, u3)) ^ te<3>(c, taddr<0>(c, u1)) ^ k2.z;
+    cc.c3 = te<0>(c, taddr<3>(c, u3)) ^ te<2>(c, taddr<1>(c, u1)) ^ te<3>(c, taddr<0>(c, u2)) ^ k2.w;
   }
   const uint32_t a0 = cc.k0 ^ te<3>(c, taddr<0>(c, w3));
   uint32_t s0 = cc.c0 ^ te<0>(c, taddr<3>(c, a0)), s1 = cc.c1 ^ te<3>(c, taddr<0>(c, a0));

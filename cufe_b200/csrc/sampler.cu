@@ -19,6 +19,7 @@
 #include "prof.h"
 
 #include <algorithm>
+#include <cmath>
 
 namespace cufe {
 
@@ -44,7 +45,7 @@ __device__ __noinline__ void ctr_block_g(uint32_t (&W)[4], uint32_t ctr, const u
 // 1 - 7 K / 2^32 = 0.84%; far less for sigma_1): rescan bytes 200.. with the rejection loop of
 // src/gauss.c:578-703, regenerating blocks as needed
 template <int SIG>
-__device__ __noinline__ void uniform_slow(uint32_t *y, uint32_t cb, const uint32_t *__restrict__ rkg,
+__device__ __noinline__ void uniform_slow(uint32_t *y, int ystride, uint32_t cb, const uint32_t *__restrict__ rkg,
                                           const AesCtx &c, uint32_t *status) {
   int w = 0, have_blk = -1;
   uint32_t W[4] = {0, 0, 0, 0};
@@ -66,7 +67,7 @@ __device__ __noinline__ void uniform_slow(uint32_t *y, uint32_t cb, const uint32
       ++w;
       if (uniform_ok<SIG>(x)) break;
     }
-    y[j] = uniform_reduce<SIG>(x);
+    y[j * ystride] = uniform_reduce<SIG>(x);
   }
 }
 
@@ -100,16 +101,49 @@ __device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb,
 // word 70): 13 of the refill's 24 blocks.  Blocks 0, 1, 7 hold only the low CDT words, which
 // S1/S2 never use and S3 uses only on ties; blocks 15 and 16 hold uniform words 60..67, needed
 // only when fewer than 8 of the first 10 words are accepted.  Both rare cases regenerate what
-// they need on their slow paths.  Buffer word kbuf(w) holds refill word w.
+// they need on their slow paths.
+//
+// The blocks are computed in the order below and each is consumed as soon as it exists, so a
+// refill never buffers its keystream: the uniform words and the sign byte first (every
+// candidate needs its y and sign bit), then the exponent word of lanes 0..3, and from there
+// every CDT sample and every candidate the moment its last word arrives.  All live values
+// (the 8 y, the packed CDT samples, a few words carried to the next block, the outputs) are
+// registers; a buffered keystream had to live in local memory, whose traffic took 6% of the
+// L1 data pipe that the table lookups saturate and missed L1 on a third of its loads.
 constexpr int kRefillBlocks = 13;
-__constant__ uint8_t c_refill_blocks[kRefillBlocks] = {2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, 17};
-__host__ __device__ constexpr int kbuf(int w) { return w < 28 ? w - 8 : (w < 60 ? w - 12 : w - 20); }
-static_assert(kbuf(70) == 4 * 12 + 2, "sign word lives in block 17, the last buffer block");
-static_assert(kbuf(59) == 4 * 11 + 3, "uniform words end in block 14");
-static_assert(kbuf(49) == 4 * 9 + 1 && kbuf(50) == 4 * 9 + 2, "block 12 holds words 48..51");
+__constant__ uint8_t c_refill_order[kRefillBlocks] = {12, 13, 14, 17, 6, 2, 3, 4, 5, 8, 9, 10, 11};
 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
-constexpr int kUniformWords = 10;  // words scanned branch-free (blocks 12..14); more with p ~ 7e-5
+
+// one uniform word of the branch-free scan (src/gauss.c:578-703): the first 8 accepted words
+// from byte 200 become y[0..7] (registers: the same 8 words in a shared-memory slot measured
+// 17% slower on the whole kernel)
+template <int SIG>
+__device__ __forceinline__ void uniform_step(uint32_t (&y)[8], uint32_t &cnt, uint32_t be_word) {
+  const uint32_t v = bswap32(be_word);
+  const bool ok = uniform_ok<SIG>(v) && cnt < 8;
+  const uint32_t r = uniform_reduce<SIG>(v);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) y[j] = (ok && cnt == (uint32_t)j) ? r : y[j];
+  cnt += ok ? 1u : 0u;
+}
+
+// Candidate ln of the refill (src/gauss.c:836-890): CDT sample x (packed 4 bits per lane in
+// xp), uniform y, Bernoulli words rm (bytes 64 + 8 li + 100 h) and exponent byte, sign bit ln
+// of k8.  |value| = z < 8K < 2^33 is kept as its low word (returned) and, in `bits`, its accept
+// bit (bit ln), its bit 32 (bit 8 + ln) and bit 16 if an accepted z ever reaches 2^33.
+template <int SIG, int VAR>
+__device__ __forceinline__ uint32_t refill_candidate(int ln, uint32_t xp, uint32_t y, uint32_t rm_lo,
+                                                     uint32_t rm_hi, uint32_t ewrd, uint32_t k8, double kinv,
+                                                     uint32_t &bits) {
+  const uint32_t x = (xp >> (4 * ln)) & 15u;
+  const uint32_t rexp = (ewrd >> (24 - 8 * (ln & 3))) & 0xffu;
+  uint64_t z;
+  const bool b = candidate<SIG, VAR>(x, y, le64_of(rm_lo, rm_hi), rexp, kinv, z);
+  const uint32_t a = accept_final(b, z, (k8 >> ln) & 1u);
+  bits |= (a << ln) | ((uint32_t)((z >> 32) & 1u) << (8 + ln)) | ((a & (uint32_t)((z >> 33) != 0)) << 16);
+  return (uint32_t)z;
+}
 
 template <int SIG, bool FULL, int VAR>
 __global__ void __launch_bounds__(kCandThreads, 1)
@@ -125,76 +159,97 @@ __global__ void __launch_bounds__(kCandThreads, 1)
   uint32_t st = 0;
   uint32_t lo = 1, hi = 0;  // refill range of stream st (empty: forces the first lookup)
   CtrCache cc;
-  const uint32_t *rkg = rkeys;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     if (g < lo || g >= hi) {
       st = seg_find(sg.roff, sg.nstreams, g);
       lo = (uint32_t)__ldg(sg.roff + st);
       hi = (uint32_t)__ldg(sg.roff + st + 1);
-      rkg = rkeys + (size_t)st * 60;
 #pragma unroll
-      for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkg + i);
+      for (int i = 0; i < 60; ++i) rk[i] = __ldg(rkeys + (size_t)st * 60 + i);
       ctr_cache_key(cc, rk, c);
     }
+    const uint32_t *rkg = rkeys + (size_t)st * 60;  // the key schedule again, for rare paths
     const uint32_t t = g - lo;
     const uint32_t cb = t * 24u;
-    // 1. the keystream blocks, one AES body (keeps the loop inside the instruction cache)
-    uint4 buf4[kRefillBlocks];
-#pragma unroll 1
-    for (int bi = 0; bi < kRefillBlocks; ++bi) {
-      uint32_t W[4];
-      aes256_ctr_block_cached(W, cb + c_refill_blocks[bi], rk, c, cc);
-      buf4[bi] = make_uint4(W[0], W[1], W[2], W[3]);
-    }
-    const uint32_t *buf = reinterpret_cast<const uint32_t *>(buf4);
-    // 2. uniform y: first 8 accepted words from byte 200 (src/gauss.c:578-703), branch-free
     uint32_t y[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) y[j] = 0;
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int w = 0; w < kUniformWords; ++w) {
-      const uint32_t v = bswap32(buf[kbuf(50 + w)]);
-      const bool ok = uniform_ok<SIG>(v) && cnt < 8;
-      const uint32_t r = uniform_reduce<SIG>(v);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) y[j] = (ok && cnt == (uint32_t)j) ? r : y[j];
-      cnt += ok ? 1u : 0u;
-    }
-    if (cnt < 8) uniform_slow<SIG>(y, cb, rkg, c, status);
-    uint32_t ybuf[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) ybuf[j] = y[j];
-    const uint32_t k8 = bswap32(buf[kbuf(70)]) & 0xffu;  // sign byte 280
-    // 3. the 8 candidates, one code copy: |value| = z < 8K < 2^33 as its low word, bit 32 and
-    // the sign byte
-    uint32_t acc = 0, hib = 0, wide = 0;
-    uint32_t lo8[8];
+    uint32_t cnt = 0, k8 = 0, xp = 0, w24 = 0, w48 = 0, w49 = 0, carry = 0, lo0 = 0, lo1 = 0;
+    uint32_t bits = 0;  // accept mask, bits 32 (<< 8), wide flag (bit 16)
+    // one AES body for all 13 blocks (keeps the loop inside the instruction cache); the
+    // consumer of each block is selected by the (warp-uniform) step
 #pragma unroll 1
-    for (int ln = 0; ln < 8; ++ln) {
-      const int h = ln >> 2, li = ln & 3;
-      const int w2 = 25 * h + 8 + 2 * li;   // CDT high word of this lane (byte 32 + 8 li + 100 h)
-      const int wm = 25 * h + 16 + 2 * li;  // Bernoulli mantissa (byte 64 + 8 li + 100 h)
-      const int we = 25 * h + 24;           // exponent bytes (96 + 100 h)
-      const uint64_t r2 = le64_of(buf[kbuf(w2)], buf[kbuf(w2 + 1)]);
-      const uint32_t x = cdt_lane<FULL>(ln, r2, cb, rkg, c);
-      const uint64_t rm = le64_of(buf[kbuf(wm)], buf[kbuf(wm + 1)]);
-      const uint32_t rexp = (buf[kbuf(we)] >> (24 - 8 * li)) & 0xffu;
-      uint64_t z;
-      const bool b = candidate<SIG, VAR>(x, ybuf[ln], rm, rexp, kinv, z);
-      const uint32_t k = (k8 >> ln) & 1u;
-      const uint32_t a = accept_final(b, z, k);
-      acc |= a << ln;
-      lo8[ln] = (uint32_t)z;
-      hib |= (uint32_t)((z >> 32) & 1u) << ln;
-      wide |= a & (uint32_t)((z >> 33) != 0);
+    for (int step = 0; step < kRefillBlocks; ++step) {
+      uint32_t W[4];
+      aes256_ctr_block_cached(W, cb + c_refill_order[step], rk, rkg, c, cc);
+      switch (step) {
+        case 0:  // block 12: words 48 (rm high word of lane 7), 49 (exponents of lanes 4..7), 50, 51
+          w48 = W[0];
+          w49 = W[1];
+          uniform_step<SIG>(y, cnt, W[2]);
+          uniform_step<SIG>(y, cnt, W[3]);
+          break;
+        case 1:  // block 13: uniform words 52..55
+        case 2:  // block 14: uniform words 56..59
+#pragma unroll
+          for (int i = 0; i < 4; ++i) uniform_step<SIG>(y, cnt, W[i]);
+          if (step == 2 && cnt < 8) {
+            uint32_t ys[8];
+            uniform_slow<SIG>(ys, 1, cb, rkg, c, status);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) y[j] = ys[j];
+          }
+          break;
+        case 3:  // block 17: word 70 holds the sign byte 280
+          k8 = bswap32(W[2]) & 0xffu;
+          break;
+        case 4:  // block 6: word 24, the exponent bytes of lanes 0..3
+          w24 = W[0];
+          break;
+        case 5:  // block 2: CDT high words of lanes 0 (words 8, 9) and 1 (10, 11)
+          xp |= cdt_lane<FULL>(0, le64_of(W[0], W[1]), cb, rkg, c);
+          xp |= cdt_lane<FULL>(1, le64_of(W[2], W[3]), cb, rkg, c) << 4;
+          break;
+        case 6:  // block 3: lanes 2 (12, 13) and 3 (14, 15)
+          xp |= cdt_lane<FULL>(2, le64_of(W[0], W[1]), cb, rkg, c) << 8;
+          xp |= cdt_lane<FULL>(3, le64_of(W[2], W[3]), cb, rkg, c) << 12;
+          break;
+        case 7:  // block 4: Bernoulli words of lanes 0 (16, 17) and 1 (18, 19)
+          lo0 = refill_candidate<SIG, VAR>(0, xp, y[0], W[0], W[1], w24, k8, kinv, bits);
+          lo1 = refill_candidate<SIG, VAR>(1, xp, y[1], W[2], W[3], w24, k8, kinv, bits);
+          break;
+        case 8: {  // block 5: lanes 2 (20, 21) and 3 (22, 23); candidates 0..3 complete
+          const uint32_t lo2 = refill_candidate<SIG, VAR>(2, xp, y[2], W[0], W[1], w24, k8, kinv, bits);
+          const uint32_t lo3 = refill_candidate<SIG, VAR>(3, xp, y[3], W[2], W[3], w24, k8, kinv, bits);
+          reinterpret_cast<uint4 *>(cand_lo + (size_t)g * 8)[0] = make_uint4(lo0, lo1, lo2, lo3);
+          break;
+        }
+        case 9:  // block 8: CDT words of lane 4 (33, 34); word 35 starts lane 5
+          xp |= cdt_lane<FULL>(4, le64_of(W[1], W[2]), cb, rkg, c) << 16;
+          carry = W[3];
+          break;
+        case 10:  // block 9: lanes 5 (35, 36) and 6 (37, 38); word 39 starts lane 7
+          xp |= cdt_lane<FULL>(5, le64_of(carry, W[0]), cb, rkg, c) << 20;
+          xp |= cdt_lane<FULL>(6, le64_of(W[1], W[2]), cb, rkg, c) << 24;
+          carry = W[3];
+          break;
+        case 11:  // block 10: lane 7 CDT (39, 40); Bernoulli words of lane 4 (41, 42); 43 starts lane 5
+          xp |= cdt_lane<FULL>(7, le64_of(carry, W[0]), cb, rkg, c) << 28;
+          lo0 = refill_candidate<SIG, VAR>(4, xp, y[4], W[1], W[2], w49, k8, kinv, bits);
+          carry = W[3];
+          break;
+        default: {  // block 11: Bernoulli words of lanes 5 (43, 44), 6 (45, 46), 7 (47, 48)
+          const uint32_t lo5 = refill_candidate<SIG, VAR>(5, xp, y[5], carry, W[0], w49, k8, kinv, bits);
+          const uint32_t lo6 = refill_candidate<SIG, VAR>(6, xp, y[6], W[1], W[2], w49, k8, kinv, bits);
+          const uint32_t lo7 = refill_candidate<SIG, VAR>(7, xp, y[7], W[3], w48, w49, k8, kinv, bits);
+          reinterpret_cast<uint4 *>(cand_lo + (size_t)g * 8)[1] = make_uint4(lo0, lo5, lo6, lo7);
+          break;
+        }
+      }
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(cand_lo + (size_t)g * 8);
-    dst[0] = make_uint4(lo8[0], lo8[1], lo8[2], lo8[3]);
-    dst[1] = make_uint4(lo8[4], lo8[5], lo8[6], lo8[7]);
-    amask[g] = (uint8_t)acc;
-    chs[g] = (uint16_t)(hib | (k8 << 8));
-    if (wide) atomicOr(status, kStatusWideSample);
+    amask[g] = (uint8_t)bits;
+    chs[g] = (uint16_t)(((bits >> 8) & 0xffu) | (k8 << 8));
+    if (bits & 0x10000u) atomicOr(status, kStatusWideSample);
   }
 }
 
@@ -822,14 +877,28 @@ int sampler_init_device() {
   return CUFE_OK;
 }
 
-// accepted candidates per 8-candidate refill of the CPU mapping, rounded down from oracle
-// measurements (5.44, 4.39, 3.09 for S1, S2, S3; the truncations of Q5 reject more at large K)
-static double mean_accept(int sig) { return sig == 0 ? 5.35 : (sig == 1 ? 4.3 : 3.0); }
+// Accepted candidates per 8-candidate refill of the CPU mapping, measured on the oracle over
+// 4 M AES-CTR refills per sigma: mean 5.4436 / 4.3942 / 3.0948 (+-0.0007) and variance 1.74 /
+// 1.98 / 1.90 for S1 / S2 / S3 (the uint32 truncation of src/gauss.c:849 rejects more at large
+// K).  The means below are those rounded down, the variance bound is 2.0 for all three.
+static double mean_accept(int sig) { return sig == 0 ? 5.443 : (sig == 1 ? 4.393 : 3.094); }
+constexpr double kAcceptVarBound = 2.0;
 
+// Refills precomputed for `calls` consecutive calls of n samples.  A call consumes r refills,
+// the first whose accepted total reaches n; E[r] = (n + overshoot) / mu < n / mu + 1 (the
+// overshoot averages below 1.4 samples), and over many calls sum(r) has variance about
+// calls n v / mu^3 (renewal count).  The range is calls (n / mu + 1) plus 12 of those
+// standard deviations plus 64.  Against the exact distribution of r (dynamic programming
+// over the measured accept-count histogram), that is at least 13 standard deviations of
+// sum(r) above its mean for every n in 16..8192 and 1..4096 calls, and 0.2-0.6% above the
+// mean need for long streams (the former 3% margin over rounded-down means was 6%).  A
+// stream that still ran short sets kStatusRefillsExhausted (checked by the host) and never
+// reads past its range.
 uint32_t cpu_map_refills(uint32_t calls, uint32_t n, int sig) {
-  const double mu = mean_accept(sig);
+  const double mu = mean_accept(sig), cn = (double)calls * (double)n;
   const double need = (double)calls * ((double)n / mu + 1.0);
-  uint32_t R = (uint32_t)(need * 1.03) + 256;
+  const double sd = std::sqrt(cn * kAcceptVarBound / (mu * mu * mu));
+  const uint32_t R = (uint32_t)std::ceil(need + 12.0 * sd) + 64;
   return (R + 31) & ~31u;
 }
 
