@@ -90,8 +90,10 @@ __device__ __noinline__ uint32_t cdt_full_slow(int lane, uint64_t r2, uint32_t c
 template <bool FULL>
 __device__ __forceinline__ uint32_t cdt_lane(int lane, uint64_t r2, uint32_t cb, const uint32_t *rkg,
                                              const AesCtx &c) {
-  if (FULL && cdt_needs_low(r2)) return cdt_full_slow(lane, r2, cb, rkg, c);
-  return cdt_sample<false>(r2, 0);
+  bool tie;
+  const uint32_t x = cdt_sample_hi(r2, tie);
+  if (FULL && tie) return cdt_full_slow(lane, r2, cb, rkg, c);
+  return x;
 }
 
 // Blocks of one refill that the fast path reads (16-byte block b = bytes 16b..16b+15, word w
@@ -118,14 +120,19 @@ constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 regi
 // one uniform word of the branch-free scan (src/gauss.c:578-703): the first 8 accepted words
 // from byte 200 become y[0..7] (registers: the same 8 words in a shared-memory slot measured
 // 17% slower on the whole kernel)
-template <int SIG>
-__device__ __forceinline__ void uniform_step(uint32_t (&y)[8], uint32_t &cnt, uint32_t be_word) {
+// Word W (0..9) of that scan.  With at most 2 of the 10 words rejected (otherwise the slow
+// path redoes the scan) word W lands in slot W - rej, rej = rejections before it, so only
+// the slots W-2..W are candidates (3 selects per word, not 8); slots past 7 are dropped as
+// the reference's loop stops at 8 accepted words.
+template <int SIG, int W>
+__device__ __forceinline__ void uniform_step(uint32_t (&y)[8], uint32_t &rej, uint32_t be_word) {
   const uint32_t v = bswap32(be_word);
-  const bool ok = uniform_ok<SIG>(v) && cnt < 8;
+  const bool ok = uniform_ok<SIG>(v);
   const uint32_t r = uniform_reduce<SIG>(v);
 #pragma unroll
-  for (int j = 0; j < 8; ++j) y[j] = (ok && cnt == (uint32_t)j) ? r : y[j];
-  cnt += ok ? 1u : 0u;
+  for (int k = 0; k < 3; ++k)
+    if (W - k >= 0 && W - k < 8) y[W - k] = (ok && rej == (uint32_t)k) ? r : y[W - k];
+  rej += ok ? 0u : 1u;
 }
 
 // Candidate ln of the refill (src/gauss.c:836-890): CDT sample x (packed 4 bits per lane in
@@ -174,7 +181,7 @@ __global__ void __launch_bounds__(kCandThreads, 1)
     uint32_t y[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) y[j] = 0;
-    uint32_t cnt = 0, k8 = 0, xp = 0, w24 = 0, w48 = 0, w49 = 0, carry = 0, lo0 = 0, lo1 = 0;
+    uint32_t rej = 0, k8 = 0, xp = 0, w24 = 0, w48 = 0, w49 = 0, carry = 0, lo0 = 0, lo1 = 0;
     uint32_t bits = 0;  // accept mask, bits 32 (<< 8), wide flag (bit 16)
     // one AES body for all 13 blocks (keeps the loop inside the instruction cache); the
     // consumer of each block is selected by the (warp-uniform) step
@@ -186,14 +193,21 @@ __global__ void __launch_bounds__(kCandThreads, 1)
         case 0:  // block 12: words 48 (rm high word of lane 7), 49 (exponents of lanes 4..7), 50, 51
           w48 = W[0];
           w49 = W[1];
-          uniform_step<SIG>(y, cnt, W[2]);
-          uniform_step<SIG>(y, cnt, W[3]);
+          uniform_step<SIG, 0>(y, rej, W[2]);
+          uniform_step<SIG, 1>(y, rej, W[3]);
           break;
         case 1:  // block 13: uniform words 52..55
-        case 2:  // block 14: uniform words 56..59
-#pragma unroll
-          for (int i = 0; i < 4; ++i) uniform_step<SIG>(y, cnt, W[i]);
-          if (step == 2 && cnt < 8) {
+          uniform_step<SIG, 2>(y, rej, W[0]);
+          uniform_step<SIG, 3>(y, rej, W[1]);
+          uniform_step<SIG, 4>(y, rej, W[2]);
+          uniform_step<SIG, 5>(y, rej, W[3]);
+          break;
+        case 2:  // block 14: uniform words 56..59; fewer than 8 of the 10 accepted: slow path
+          uniform_step<SIG, 6>(y, rej, W[0]);
+          uniform_step<SIG, 7>(y, rej, W[1]);
+          uniform_step<SIG, 8>(y, rej, W[2]);
+          uniform_step<SIG, 9>(y, rej, W[3]);
+          if (rej > 2) {
             uint32_t ys[8];
             uniform_slow<SIG>(ys, 1, cb, rkg, c, status);
 #pragma unroll

@@ -13,13 +13,22 @@ __host__ __device__ constexpr uint64_t sigma_k(int sig) {
 }
 
 // CDT of the base sampler, (low63, high63) of P(x > i) (src/gauss.c:63-73); kept identical
-// because every sample bit depends on it.
+// because every sample bit depends on it.  The high words are also compile-time constants
+// (cdt_hi) for the fast path, where two of them are zero and the rest become immediates.
+__host__ __device__ constexpr uint64_t cdt_hi(int i) {
+  return i == 0 ? 3327841033070651387ull
+         : i == 1 ? 380075531178589176ull
+         : i == 2 ? 11604843442081400ull
+         : i == 3 ? 90134450315532ull
+         : i == 4 ? 175786317361ull
+         : i == 5 ? 85801740ull
+         : i == 6 ? 10472ull
+                  : 0ull;
+}
 static __constant__ uint64_t c_cdt[9][2] = {
-    {2200310400551559144ull, 3327841033070651387ull}, {7912151619254726620ull, 380075531178589176ull},
-    {5167367257772081627ull, 11604843442081400ull},   {5081592746475748971ull, 90134450315532ull},
-    {6522074513864805092ull, 175786317361ull},        {2579734681240182346ull, 85801740ull},
-    {8175784047440310133ull, 10472ull},               {2947787991558061753ull, 0ull},
-    {22489665999543ull, 0ull}};
+    {2200310400551559144ull, cdt_hi(0)}, {7912151619254726620ull, cdt_hi(1)}, {5167367257772081627ull, cdt_hi(2)},
+    {5081592746475748971ull, cdt_hi(3)}, {6522074513864805092ull, cdt_hi(4)}, {2579734681240182346ull, cdt_hi(5)},
+    {8175784047440310133ull, cdt_hi(6)}, {2947787991558061753ull, cdt_hi(7)}, {22489665999543ull, cdt_hi(8)}};
 // 2^f polynomial (src/gauss.c:102-111), kept identical (the Bernoulli compares its bits)
 static __constant__ uint64_t c_expc[10] = {0x3e833b70ffa2c5d4ull, 0x3eb4a480fda7e6e1ull, 0x3ef01b254493363full,
                                     0x3f242e0e0aa273ccull, 0x3f55d8a2334ed31bull, 0x3f83b2aa56db0f1aull,
@@ -54,13 +63,20 @@ __device__ __forceinline__ uint32_t cdt_sample(uint64_t r2, uint64_t r1) {
   }
   return x;
 }
-// FULL compare needs the low words only when the high word ties a table entry
-__device__ __forceinline__ bool cdt_needs_low(uint64_t r2) {
+// The high-word compare of cdt_sample<false> from the constant high words, and whether r2
+// ties one of them (the FULL compare needs the low words only then), from the same
+// differences.
+__device__ __forceinline__ uint32_t cdt_sample_hi(uint64_t r2, bool &tie) {
   r2 &= 0x7fffffffffffffffull;
-  bool t = false;
+  uint32_t x = 0;
+  tie = false;
 #pragma unroll
-  for (int i = 0; i < 9; ++i) t |= (r2 == c_cdt[i][1]);
-  return t;
+  for (int i = 0; i < 9; ++i) {
+    const uint64_t d = r2 - cdt_hi(i);
+    x += (uint32_t)(d >> 63);
+    tie |= d == 0;
+  }
+  return x;
 }
 
 // Bernoulli variants (see oracle/cufe_oracle.c bernoulli_lane for the derivation):
