@@ -117,13 +117,12 @@ __constant__ uint8_t c_refill_order[kRefillBlocks] = {12, 13, 14, 17, 6, 2, 3, 4
 
 constexpr int kCandThreads = 512;  // 1 CTA (128 KiB of tables) per SM; 128 registers per thread
 
-// one uniform word of the branch-free scan (src/gauss.c:578-703): the first 8 accepted words
-// from byte 200 become y[0..7] (registers: the same 8 words in a shared-memory slot measured
-// 17% slower on the whole kernel)
-// Word W (0..9) of that scan.  With at most 2 of the 10 words rejected (otherwise the slow
-// path redoes the scan) word W lands in slot W - rej, rej = rejections before it, so only
-// the slots W-2..W are candidates (3 selects per word, not 8); slots past 7 are dropped as
-// the reference's loop stops at 8 accepted words.
+// Word W (0..9) of the branch-free uniform scan (src/gauss.c:578-703): the first 8 accepted
+// words from byte 200 become y[0..7], kept in registers (the same 8 words in a shared-memory
+// slot measured 17% slower on the whole kernel).  With at most 2 of the 10 words rejected
+// (otherwise the slow path redoes the scan) word W lands in slot W - rej, rej = rejections
+// before it, so only the slots W-2..W are candidates (3 selects per word, not 8); slots past
+// 7 are dropped, as the reference's loop stops at 8 accepted words.
 template <int SIG, int W>
 __device__ __forceinline__ void uniform_step(uint32_t (&y)[8], uint32_t &rej, uint32_t be_word) {
   const uint32_t v = bswap32(be_word);
